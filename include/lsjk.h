@@ -1,0 +1,145 @@
+/*
+ * lsjk.h -- C ABI of the B200 Coulomb/exchange (J/K) engine.
+ *
+ * This is the boundary the Lightspeed IntBox J/K path binds to. It replaces the
+ * closed TeraChem library behind IntBox::coulombTC / exchangeTC
+ * (src/cpp/intbox/tc/coulomb.cpp:14-63, tc/exchange.cpp:14-77 in the reference)
+ * and is called from the C++ IntBox::coulomb / IntBox::exchange shim in
+ * lightspeed_b200/csrc/host/intbox.cpp, which keeps the reference signatures
+ * (src/lightspeed/intbox.hpp:761-771 and :817-828).
+ *
+ * Conventions
+ *  - Plain C types only; every function returns 0 on success and a nonzero
+ *    LSJK_E* code on failure, with a message from lsjk_last_error() (per
+ *    thread). No entry point falls back to the CPU.
+ *  - Matrices are dense row-major double arrays in the basis' AO ("pure")
+ *    representation, exactly the Lightspeed Tensor layout (src/lightspeed/
+ *    tensor.hpp:19-320). Results are ACCUMULATED into the caller's arrays, as
+ *    IntBox::coulomb/exchange do when J12/K13 is passed in.
+ *  - Host-pointer entry points copy in and out on the context's stream and
+ *    return after the result is in host memory. The *_device entry points take
+ *    device pointers and only enqueue work on the context's stream.
+ *  - A context is not reentrant: one caller thread at a time (the reference's
+ *    TCIntBox session has the same rule, tc/tcintbox/tcintbox.cpp:75-78).
+ */
+#ifndef LSJK_H
+#define LSJK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSJK_OK            0
+#define LSJK_EINVAL        1   /* bad argument / shape / unsupported basis    */
+#define LSJK_ECUDA         2   /* CUDA runtime error                          */
+#define LSJK_ENOMEM        3   /* device allocation failed                    */
+#define LSJK_EKERNEL       4   /* a kernel reported an error status           */
+#define LSJK_ENOTSUPP      5   /* angular momentum beyond the built kernels   */
+
+/* Precision policy (reference semantics, src/lightspeed/intbox.hpp:730-740):
+ * quartets whose estimate is >= thredp run in FP64, those in [thresp, thredp)
+ * in FP32 (LSJK_PREC_MIXED); LSJK_PREC_FP64 runs every quartet >= thresp in
+ * FP64, like the reference CPU path. Accumulation is always FP64. */
+#define LSJK_PREC_MIXED 0
+#define LSJK_PREC_FP64  1
+
+typedef struct lsjk_context  lsjk_context;
+typedef struct lsjk_basis    lsjk_basis;
+typedef struct lsjk_pairlist lsjk_pairlist;
+
+/* Work counters accumulated since the context was created or last reset.
+ * Quartets are primitive quartets that passed the screen (counted once per
+ * quartet, whatever the number of Ewald terms); flops are algorithmic flops
+ * per quartet class x quartets (one Ewald term). */
+typedef struct lsjk_stats {
+    double quartets_fp64;      /* primitive quartets evaluated in FP64 (J + K) */
+    double quartets_fp32;      /* ... in FP32                                  */
+    double j_quartets;         /* J quartets (both precisions)                 */
+    double k_quartets;         /* K quartets (both precisions)                 */
+    double ms_j;               /* reserved (0)                                 */
+    double ms_k;               /* reserved (0)                                 */
+    double flops_j;            /* algorithmic flops of the J quartets          */
+    double flops_k;            /* algorithmic flops of the K quartets          */
+    long   kernel_launches;    /* kernels launched (host count)                */
+} lsjk_stats;
+
+/* Last error message of the calling thread ("" if none). */
+const char* lsjk_last_error(void);
+
+/* Library version string. */
+const char* lsjk_version(void);
+
+/* ---- context: one per device; owns the stream, tables and scratch memory.
+ * Replaces the TCIntBox session (tc/tcintbox/tcintbox.cpp:20-50). */
+int lsjk_context_create(int device, lsjk_context** out);
+int lsjk_context_destroy(lsjk_context* ctx);
+int lsjk_context_set_precision(lsjk_context* ctx, int mode);
+/* The CUDA stream (cudaStream_t) the context enqueues on, as void*. */
+void* lsjk_context_stream(lsjk_context* ctx);
+int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out);
+int lsjk_context_reset_stats(lsjk_context* ctx);
+/* Copy the device status word of the context's kernels (0 = no error). */
+int lsjk_context_status(lsjk_context* ctx, int* status);
+
+/* ---- basis: primitive shells exactly as lightspeed::Primitive
+ * (src/lightspeed/basis.hpp:143-172); xyz is nprim x 3. Dense primIdx,
+ * aoIdx, cartIdx, shellIdx and atomIdx are validated as in the Basis
+ * constructor (basis.hpp:433-470). */
+int lsjk_basis_create(lsjk_context* ctx, int nprim,
+                      const double* c, const double* e, const double* xyz,
+                      const int* L, const int* is_pure, const int* aoIdx,
+                      const int* cartIdx, const int* primIdx, const int* shellIdx,
+                      const int* atomIdx, lsjk_basis** out);
+int lsjk_basis_destroy(lsjk_basis* basis);
+int lsjk_basis_nao(const lsjk_basis* basis);
+int lsjk_basis_ncart(const lsjk_basis* basis);
+
+/* ---- pair list: PairList::build_schwarz (src/cpp/core/pair_list.cpp:29-177)
+ * built on the device: Schwarz bounds of all primitive pairs (pair_list.cpp:
+ * 15-27), pairs with bound > thre kept (lower triangle if symmetric), grouped
+ * by (L1, L2) and sorted by bound descending, then prim1, prim2 ascending
+ * (pair_list_util.cpp:12-20). */
+int lsjk_pairlist_build_schwarz(lsjk_context* ctx, const lsjk_basis* basis1,
+                                const lsjk_basis* basis2, int is_symmetric, float thre,
+                                lsjk_pairlist** out);
+int lsjk_pairlist_destroy(lsjk_pairlist* pl);
+long lsjk_pairlist_size(const lsjk_pairlist* pl);
+/* Copy the pairs out in class order (L1-major, then L2) and sorted order. */
+int lsjk_pairlist_export(const lsjk_pairlist* pl, int* L1, int* L2, int* prim1,
+                         int* prim2, float* bound);
+
+/* ---- J: J12 += sum_rs (pq|rs) D34_rs for the Ewald operator
+ * O(r) = sum_i scales[i] erf(omegas[i] r)/r (omega = -1: 1/r), ndens densities
+ * at once. IntBox::coulomb (src/lightspeed/intbox.hpp:761-771,
+ * src/cpp/intbox/intbox.cpp:213-250). D34[k] is (nao3, nao4), J12[k] is
+ * (nao1, nao2), host memory. */
+int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                 const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                 const double* const* D34, float thresp, float thredp, double* const* J12);
+
+/* ---- K: K13 += sum_qs (pq|rs) D24_qs with the reference's density-screened
+ * K-invert ordering. IntBox::exchange (src/lightspeed/intbox.hpp:817-828,
+ * src/cpp/intbox/intbox.cpp:290-330). D24symm requires basis 2 == basis 4
+ * (LSJK_EINVAL otherwise, like src/cpp/intbox/cpu/exchange.cpp:74-76). */
+int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                  const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                  const double* const* D24, int D24symm, float thresp, float thredp,
+                  double* const* K13);
+
+/* Device-resident variants: D and J/K are device pointers (same layout); the
+ * work is only enqueued on the context stream. Used when the caller keeps its
+ * matrices in HBM across SCF iterations. */
+int lsjk_coulomb_device(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                        const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                        const double* const* D34_dev, float thresp, float thredp,
+                        double* const* J12_dev);
+int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                         const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                         const double* const* D24_dev, int D24symm, float thresp, float thredp,
+                         double* const* K13_dev);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LSJK_H */

@@ -1,0 +1,434 @@
+// extern "C" entry points of liblsjk.so (declared in include/lsjk.h).
+#include <cstring>
+#include <string>
+#include <vector>
+#include "engine.cuh"
+#include "lsjk_device.cuh"
+
+struct lsjk_context { lsjk::Context c; };
+struct lsjk_basis { lsjk::Basis b; };
+struct lsjk_pairlist { lsjk::PairList p; };
+
+namespace lsjk {
+void basis_init(Context* ctx, Basis* B);
+}
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guard(F&& f)
+{
+    try {
+        f();
+        g_err.clear();
+        return LSJK_OK;
+    } catch (const lsjk::Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return LSJK_EINVAL;
+    }
+}
+
+void set_device(const lsjk::Context& c) { LSJK_CUDA(cudaSetDevice(c.device)); }
+
+lsjk::Ewald make_ewald(int nterm, const double* scales, const double* omegas)
+{
+    if (nterm < 1 || !scales || !omegas) throw lsjk::Error(LSJK_EINVAL, "Ewald: need >= 1 term");
+    lsjk::Ewald ew;
+    for (int t = 0; t < nterm; ++t) {
+        // terms with zero scale or zero omega contribute nothing (coulomb.cpp:72-73)
+        if (scales[t] == 0.0 || omegas[t] == 0.0) continue;
+        ew.alpha.push_back(scales[t]);
+        ew.omega.push_back(omegas[t]);
+    }
+    if (ew.alpha.size() > 4) throw lsjk::Error(LSJK_EINVAL, "Ewald: at most 4 nonzero terms are supported");
+    return ew;
+}
+
+void check_kernels(lsjk::Context* ctx)
+{
+    int st = 0;
+    LSJK_CUDA(cudaMemcpyAsync(&st, ctx->status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    LSJK_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (st) {
+        LSJK_CUDA(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->stream));
+        throw lsjk::Error(LSJK_EKERNEL, "a J/K kernel reported error status " + std::to_string(st));
+    }
+}
+
+void check_lmax(const lsjk::PairList* pl)
+{
+    if (pl->b1->maxL > lsjk::kLmax || pl->b2->maxL > lsjk::kLmax)
+        throw lsjk::Error(LSJK_ENOTSUPP, "J/K: angular momentum above d is not supported by the GPU kernels");
+}
+
+// One J or K build for one density, device pointers in and out.
+void coulomb_one(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
+                 const lsjk::PairList* pl34, const double* Dpure, double* Jpure, float thresp, float thredp)
+{
+    ctx->scratch_reset();
+    const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    double* Dc = lsjk::take<double>(ctx, (size_t) b3->ncart * b4->ncart);
+    double* Jc = lsjk::take<double>(ctx, (size_t) b1->ncart * b2->ncart);
+    lsjk::pure_to_cart(ctx, b3, b4, Dpure, Dc);
+    LSJK_CUDA(cudaMemsetAsync(Jc, 0, sizeof(double) * b1->ncart * b2->ncart, ctx->stream));
+    if (!ew.alpha.empty() && pl12->npair && pl34->npair)
+        lsjk::coulomb_build(ctx, ew, pl12, pl34, Dc, Jc, thresp, thredp);
+    lsjk::cart_to_pure_acc(ctx, b1, b2, Jc, Jpure);
+}
+
+void exchange_one(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
+                  const lsjk::PairList* pl34, const double* Dpure, bool d24symm, bool flip_ok,
+                  double* Kpure, float thresp, float thredp)
+{
+    ctx->scratch_reset();
+    const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    double* Dc = lsjk::take<double>(ctx, (size_t) b2->ncart * b4->ncart);
+    double* Kc = lsjk::take<double>(ctx, (size_t) b1->ncart * b3->ncart);
+    lsjk::pure_to_cart(ctx, b2, b4, Dpure, Dc);
+    LSJK_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * b1->ncart * b3->ncart, ctx->stream));
+    if (!ew.alpha.empty() && pl12->npair && pl34->npair)
+        lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Kc, d24symm, flip_ok, thresp, thredp);
+    lsjk::cart_to_pure_acc(ctx, b1, b3, Kc, Kpure);
+}
+
+void exchange_prepare(lsjk::Context* ctx, lsjk::PairList* pl12, lsjk::PairList* pl34, int D24symm,
+                      bool* d24, bool* flip)
+{
+    check_lmax(pl12);
+    check_lmax(pl34);
+    bool symm = D24symm != 0;
+    if (symm && !pl12->b2->equivalent(*pl34->b2))
+        throw lsjk::Error(LSJK_EINVAL,
+                          "IntBox::exchange: D24symm implied, but basis sets 2 and 4 not the same");
+    *d24 = symm;
+    // the transposed write needs basis 1 == basis 3 as well (exchange.cpp:79-81)
+    *flip = symm && pl12->b1->equivalent(*pl34->b1);
+    *d24 = *flip;
+    lsjk::build_kinv(ctx, pl12);
+    if (pl34 != pl12) lsjk::build_kinv(ctx, pl34);
+}
+
+} // namespace
+
+extern "C" {
+
+const char* lsjk_last_error(void) { return g_err.c_str(); }
+
+const char* lsjk_version(void) { return "lsjk 0.1 (sm_100a)"; }
+
+int lsjk_context_create(int device, lsjk_context** out)
+{
+    return guard([&] {
+        if (!out) throw lsjk::Error(LSJK_EINVAL, "null output");
+        auto* h = new lsjk_context();
+        lsjk::Context& c = h->c;
+        try {
+            c.device = device;
+            LSJK_CUDA(cudaSetDevice(device));
+            LSJK_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            std::vector<double> boys(kBoysCoef, kBoysCoef + sizeof(kBoysCoef) / sizeof(double));
+            std::vector<double> rys(kRysCoef, kRysCoef + sizeof(kRysCoef) / sizeof(double));
+            std::vector<double> asym(kRysAsymT, kRysAsymT + sizeof(kRysAsymT) / sizeof(double));
+            asym.insert(asym.end(), kRysAsymW, kRysAsymW + sizeof(kRysAsymW) / sizeof(double));
+            c.boys64.upload(boys, c.stream);
+            c.rys64.upload(rys, c.stream);
+            c.rys_asym64.upload(asym, c.stream);
+            c.boys32.upload(std::vector<float>(boys.begin(), boys.end()), c.stream);
+            c.rys32.upload(std::vector<float>(rys.begin(), rys.end()), c.stream);
+            c.rys_asym32.upload(std::vector<float>(asym.begin(), asym.end()), c.stream);
+            c.status.alloc(1);
+            LSJK_CUDA(cudaMemsetAsync(c.status.p, 0, sizeof(int), c.stream));
+            c.counters.alloc(lsjk::kNCounters);
+            LSJK_CUDA(cudaMemsetAsync(c.counters.p, 0, sizeof(unsigned long long) * lsjk::kNCounters, c.stream));
+            LSJK_CUDA(cudaEventCreate(&c.ev0));
+            LSJK_CUDA(cudaEventCreate(&c.ev1));
+            LSJK_CUDA(cudaEventCreate(&c.ev2));
+            LSJK_CUDA(cudaStreamSynchronize(c.stream));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int lsjk_context_destroy(lsjk_context* ctx)
+{
+    return guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->c.device);
+        cudaStreamSynchronize(ctx->c.stream);
+        if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);
+        if (ctx->c.ev1) cudaEventDestroy(ctx->c.ev1);
+        if (ctx->c.ev2) cudaEventDestroy(ctx->c.ev2);
+        cudaStream_t s = ctx->c.stream;
+        delete ctx;
+        if (s) cudaStreamDestroy(s);
+    });
+}
+
+int lsjk_context_set_precision(lsjk_context* ctx, int mode)
+{
+    return guard([&] {
+        if (!ctx || (mode != LSJK_PREC_MIXED && mode != LSJK_PREC_FP64))
+            throw lsjk::Error(LSJK_EINVAL, "bad precision mode");
+        ctx->c.precision = mode;
+    });
+}
+
+void* lsjk_context_stream(lsjk_context* ctx) { return ctx ? (void*) ctx->c.stream : nullptr; }
+
+int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out)
+{
+    return guard([&] {
+        if (!ctx || !out) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context& c = ctx->c;
+        set_device(c);
+        std::vector<unsigned long long> h(lsjk::kNCounters);
+        LSJK_CUDA(cudaMemcpyAsync(h.data(), c.counters.p, sizeof(unsigned long long) * h.size(),
+                                  cudaMemcpyDeviceToHost, c.stream));
+        LSJK_CUDA(cudaStreamSynchronize(c.stream));
+        lsjk_stats st = c.stats;
+        st.quartets_fp64 = st.quartets_fp32 = st.j_quartets = st.k_quartets = st.flops_j = st.flops_k = 0.0;
+        for (int prec = 0; prec < 2; ++prec) {
+            const unsigned long long* b = h.data() + prec * (lsjk::kNJClass + lsjk::kNKClass);
+            for (int LB = 0; LB < lsjk::kNHerm; ++LB)
+                for (int LK = 0; LK < lsjk::kNHerm; ++LK) {
+                    double n = (double) b[LB * lsjk::kNHerm + LK];
+                    st.j_quartets += n;
+                    (prec ? st.quartets_fp32 : st.quartets_fp64) += n;
+                    st.flops_j += n * lsjk::j_quartet_flops(LB, LK);
+                }
+            for (int L1 = 0; L1 < lsjk::kNL; ++L1)
+                for (int L2 = 0; L2 < lsjk::kNL; ++L2)
+                    for (int L3 = 0; L3 < lsjk::kNL; ++L3)
+                        for (int L4 = 0; L4 < lsjk::kNL; ++L4) {
+                            int ci = ((L1 * lsjk::kNL + L2) * lsjk::kNL + L3) * lsjk::kNL + L4;
+                            double n = (double) b[lsjk::kNJClass + ci];
+                            st.k_quartets += n;
+                            (prec ? st.quartets_fp32 : st.quartets_fp64) += n;
+                            st.flops_k += n * lsjk::k_quartet_flops(L1, L2, L3, L4);
+                        }
+        }
+        *out = st;
+    });
+}
+
+int lsjk_context_reset_stats(lsjk_context* ctx)
+{
+    return guard([&] {
+        if (!ctx) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        LSJK_CUDA(cudaMemsetAsync(ctx->c.counters.p, 0, sizeof(unsigned long long) * lsjk::kNCounters,
+                                  ctx->c.stream));
+        LSJK_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        ctx->c.stats = lsjk_stats{};
+    });
+}
+
+int lsjk_context_status(lsjk_context* ctx, int* status)
+{
+    return guard([&] {
+        if (!ctx || !status) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        LSJK_CUDA(cudaMemcpyAsync(status, ctx->c.status.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->c.stream));
+        LSJK_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int lsjk_basis_create(lsjk_context* ctx, int nprim, const double* c, const double* e, const double* xyz,
+                      const int* L, const int* is_pure, const int* aoIdx, const int* cartIdx,
+                      const int* primIdx, const int* shellIdx, const int* atomIdx, lsjk_basis** out)
+{
+    return guard([&] {
+        if (!ctx || !out || nprim < 0) throw lsjk::Error(LSJK_EINVAL, "bad basis arguments");
+        if (nprim > 0 && (!c || !e || !xyz || !L || !is_pure || !aoIdx || !cartIdx || !primIdx ||
+                          !shellIdx || !atomIdx))
+            throw lsjk::Error(LSJK_EINVAL, "null basis array");
+        set_device(ctx->c);
+        auto* h = new lsjk_basis();
+        lsjk::Basis& B = h->b;
+        B.ctx = &ctx->c;
+        B.nprim = nprim;
+        B.c.assign(c, c + nprim);
+        B.e.assign(e, e + nprim);
+        for (int i = 0; i < nprim; ++i) {
+            B.x.push_back(xyz[3 * i]);
+            B.y.push_back(xyz[3 * i + 1]);
+            B.z.push_back(xyz[3 * i + 2]);
+        }
+        B.L.assign(L, L + nprim);
+        B.pure.assign(is_pure, is_pure + nprim);
+        B.ao.assign(aoIdx, aoIdx + nprim);
+        B.cart.assign(cartIdx, cartIdx + nprim);
+        B.prim.assign(primIdx, primIdx + nprim);
+        B.shell.assign(shellIdx, shellIdx + nprim);
+        B.atom.assign(atomIdx, atomIdx + nprim);
+        try {
+            lsjk::basis_init(&ctx->c, &B);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int lsjk_basis_destroy(lsjk_basis* basis)
+{
+    return guard([&] { delete basis; });
+}
+
+int lsjk_basis_nao(const lsjk_basis* basis) { return basis ? basis->b.nao : -1; }
+int lsjk_basis_ncart(const lsjk_basis* basis) { return basis ? basis->b.ncart : -1; }
+
+int lsjk_pairlist_build_schwarz(lsjk_context* ctx, const lsjk_basis* basis1, const lsjk_basis* basis2,
+                                int is_symmetric, float thre, lsjk_pairlist** out)
+{
+    return guard([&] {
+        if (!ctx || !basis1 || !basis2 || !out) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        auto* h = new lsjk_pairlist();
+        lsjk::PairList& P = h->p;
+        P.ctx = &ctx->c;
+        P.b1 = &basis1->b;
+        P.b2 = &basis2->b;
+        P.symm = is_symmetric != 0;
+        P.thre = thre;
+        try {
+            lsjk::build_pairlist(&ctx->c, &P);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int lsjk_pairlist_destroy(lsjk_pairlist* pl)
+{
+    return guard([&] { delete pl; });
+}
+
+long lsjk_pairlist_size(const lsjk_pairlist* pl) { return pl ? pl->p.npair : -1; }
+
+int lsjk_pairlist_export(const lsjk_pairlist* pl, int* L1, int* L2, int* prim1, int* prim2, float* bound)
+{
+    return guard([&] {
+        if (!pl) throw lsjk::Error(LSJK_EINVAL, "null pair list");
+        const lsjk::PairList& P = pl->p;
+        long n = P.npair;
+        if (!n) return;
+        lsjk::Context* ctx = P.ctx;
+        set_device(*ctx);
+        if (prim1) LSJK_CUDA(cudaMemcpyAsync(prim1, P.p1.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        if (prim2) LSJK_CUDA(cudaMemcpyAsync(prim2, P.p2.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        if (bound) LSJK_CUDA(cudaMemcpyAsync(bound, P.bound.p, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        LSJK_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (size_t c = 0; c + 1 < P.cls_off.size(); ++c)
+            for (long k = P.cls_off[c]; k < P.cls_off[c + 1]; ++k) {
+                if (L1) L1[k] = P.cls_L1[c];
+                if (L2) L2[k] = P.cls_L2[c];
+            }
+    });
+}
+
+int lsjk_coulomb_device(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                        const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                        const double* const* D34, float thresp, float thredp, double* const* J12)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34 || ndens < 0 || (ndens && (!D34 || !J12)))
+            throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        check_lmax(&pl12->p);
+        check_lmax(&pl34->p);
+        for (int k = 0; k < ndens; ++k)
+            coulomb_one(&ctx->c, ew, &pl12->p, &pl34->p, D34[k], J12[k], thresp, thredp);
+    });
+}
+
+int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                         const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                         const double* const* D24, int D24symm, float thresp, float thredp,
+                         double* const* K13)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34 || ndens < 0 || (ndens && (!D24 || !K13)))
+            throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        bool d24 = false, flip = false;
+        exchange_prepare(&ctx->c, const_cast<lsjk::PairList*>(&pl12->p), const_cast<lsjk::PairList*>(&pl34->p),
+                         D24symm, &d24, &flip);
+        for (int k = 0; k < ndens; ++k)
+            exchange_one(&ctx->c, ew, &pl12->p, &pl34->p, D24[k], d24, flip, K13[k], thresp, thredp);
+    });
+}
+
+int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                 const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                 const double* const* D34, float thresp, float thredp, double* const* J12)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34 || ndens < 0 || (ndens && (!D34 || !J12)))
+            throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        check_lmax(&pl12->p);
+        check_lmax(&pl34->p);
+        const size_t nD = (size_t) pl34->p.b1->nao * pl34->p.b2->nao;
+        const size_t nJ = (size_t) pl12->p.b1->nao * pl12->p.b2->nao;
+        lsjk::DBuf<double> dD, dJ;
+        dD.alloc(nD);
+        dJ.alloc(nJ);
+        std::vector<double> hJ(nJ);
+        for (int k = 0; k < ndens; ++k) {
+            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p, D34[k], sizeof(double) * nD, cudaMemcpyHostToDevice, c->stream));
+            if (nJ) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * nJ, c->stream));
+            coulomb_one(c, ew, &pl12->p, &pl34->p, dD.p, dJ.p, thresp, thredp);
+            if (nJ) LSJK_CUDA(cudaMemcpyAsync(hJ.data(), dJ.p, sizeof(double) * nJ, cudaMemcpyDeviceToHost, c->stream));
+            check_kernels(c);
+            for (size_t i = 0; i < nJ; ++i) J12[k][i] += hJ[i];
+        }
+    });
+}
+
+int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                  const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
+                  const double* const* D24, int D24symm, float thresp, float thredp, double* const* K13)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34 || ndens < 0 || (ndens && (!D24 || !K13)))
+            throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        bool d24 = false, flip = false;
+        exchange_prepare(c, const_cast<lsjk::PairList*>(&pl12->p), const_cast<lsjk::PairList*>(&pl34->p), D24symm,
+                         &d24, &flip);
+        const size_t nD = (size_t) pl12->p.b2->nao * pl34->p.b2->nao;
+        const size_t nK = (size_t) pl12->p.b1->nao * pl34->p.b1->nao;
+        lsjk::DBuf<double> dD, dK;
+        dD.alloc(nD);
+        dK.alloc(nK);
+        std::vector<double> hK(nK);
+        for (int k = 0; k < ndens; ++k) {
+            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p, D24[k], sizeof(double) * nD, cudaMemcpyHostToDevice, c->stream));
+            if (nK) LSJK_CUDA(cudaMemsetAsync(dK.p, 0, sizeof(double) * nK, c->stream));
+            exchange_one(c, ew, &pl12->p, &pl34->p, dD.p, d24, flip, dK.p, thresp, thredp);
+            if (nK) LSJK_CUDA(cudaMemcpyAsync(hK.data(), dK.p, sizeof(double) * nK, cudaMemcpyDeviceToHost, c->stream));
+            check_kernels(c);
+            for (size_t i = 0; i < nK; ++i) K13[k][i] += hK[i];
+        }
+    });
+}
+
+} // extern "C"

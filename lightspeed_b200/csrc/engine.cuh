@@ -1,0 +1,221 @@
+// Internal data structures of the B200 J/K engine (not part of the C ABI).
+//
+// Device memory layout (all arrays in HBM, one allocation each):
+//  * Basis: per-primitive SoA (c, e, x, y, z, L, cartIdx, ...), plus the
+//    pure<->Cartesian maps of its shells as CSR rows.
+//  * PairList: the Schwarz-screened primitive pairs sorted exactly like the
+//    reference PairList (class (L1,L2), bound desc, prim1 asc, prim2 asc).
+//    Two derived views are kept next to it:
+//      - JBra: pairs merged by Hermite angular momentum L1+L2 and re-sorted by
+//        bound, with the Gaussian-product geometry (p, P) precomputed;
+//      - KInv: the reference's K-invert lists (src/cpp/core/kvec.cpp:31-232):
+//        for every "indexed" primitive, its partners sorted by bound desc, as
+//        CSR rows per (L_indexed, L_partner) class, with the partner data
+//        (K_ab prefactor, exponent, centre, cartIdx, bound) in SoA.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+#include <memory>
+#include <stdexcept>
+#include <cuda_runtime.h>
+#include "../../include/lsjk.h"
+
+namespace lsjk {
+
+constexpr int kLmax = 2;                       // s, p, d shells (generated kernels)
+constexpr int kNL = kLmax + 1;
+constexpr int kNHerm = 2 * kLmax + 1;          // Hermite classes L1+L2 = 0..4
+
+inline int ncart_count(int L) { return (L + 1) * (L + 2) / 2; }
+
+// Layout of the context's device counters: quartets per class, per precision.
+constexpr int kNJClass = kNHerm * kNHerm;            // (LB, LK)
+constexpr int kNKClass = kNL * kNL * kNL * kNL;      // (L1, L2, L3, L4)
+constexpr int kNCounters = 2 * (kNJClass + kNKClass); // [prec][J classes, K classes]
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define LSJK_CUDA(call)                                                                    \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            throw ::lsjk::Error(LSJK_ECUDA, std::string(#call " failed: ") +              \
+                                               cudaGetErrorString(e_));                    \
+    } while (0)
+
+// Device buffer owned by RAII (freed with the context's stream-ordered pool).
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
+    ~DBuf() { release(); }
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw Error(LSJK_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+    }
+    void upload(const std::vector<T>& h, cudaStream_t s) {
+        alloc(h.size());
+        if (!h.empty()) LSJK_CUDA(cudaMemcpyAsync(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+struct Context;
+
+// Primitive data on the device (SoA).
+struct BasisView {
+    int nprim, nao, ncart;
+    const double *c, *e, *x, *y, *z;
+    const int *L, *cart, *ao;
+};
+
+struct Basis {
+    Context* ctx = nullptr;
+    int nprim = 0, nao = 0, ncart = 0, nshell = 0, natom = 0, maxL = 0;
+    bool has_pure = false;
+    // host copies
+    std::vector<double> c, e, x, y, z;
+    std::vector<int> L, pure, ao, cart, prim, shell, atom;
+    // device copies
+    DBuf<double> dc, de, dx, dy, dz;
+    DBuf<int> dL, dcart, dao;
+    // pure <-> cart maps: cart row -> (pure index, coef) and pure row -> (cart index, coef)
+    DBuf<int> c2p_off, c2p_idx, p2c_off, p2c_idx;
+    DBuf<double> c2p_w, p2c_w;
+    BasisView view() const {
+        return BasisView{nprim, nao, ncart, dc.p, de.p, dx.p, dy.p, dz.p, dL.p, dcart.p, dao.p};
+    }
+    bool equivalent(const Basis& o) const;
+};
+
+// One Hermite class (L1+L2 = LH) of a pair list, merged over (L1, L2) and
+// sorted by bound desc (prim1, prim2 asc): the bra side of J.
+struct JBraClass {
+    int n = 0;                       // pairs in the class
+    DBuf<int> p1, p2;                // primitive indices
+    DBuf<float> bound;
+    DBuf<double> geom;               // n x 4: p, Px, Py, Pz
+};
+
+// K-invert rows of one (L_indexed, L_partner) class: for every primitive of
+// the indexed basis, the [start, start+len) slice of the partner arrays.
+struct KInvClass {
+    int nent = 0;
+    DBuf<int> row_start, row_len;    // per indexed primitive (len 0: no partners)
+};
+
+// Partner entries of all K-invert rows (SoA, sorted by class, indexed prim,
+// bound desc, partner asc -- the order of kvec.cpp:17-27).
+struct KInvData {
+    long nent = 0;
+    DBuf<double> kab, pe, px, py, pz;  // K_ab prefactor, partner exponent and centre
+    DBuf<int> pcart;                   // partner cartIdx
+    DBuf<float> pbound;                // Schwarz bound of the pair
+};
+
+struct PairList {
+    Context* ctx = nullptr;
+    const Basis* b1 = nullptr;
+    const Basis* b2 = nullptr;
+    bool symm = false;
+    float thre = 0.f;
+    long npair = 0;
+    // sorted pairs (reference order)
+    DBuf<int> p1, p2;
+    DBuf<float> bound;
+    std::vector<int> cls_L1, cls_L2;   // class list in order
+    std::vector<long> cls_off;         // offsets into the sorted arrays (size nclass+1)
+    std::vector<float> cls_max;        // first (largest) bound of each class
+    double max_bound = 0.0;            // PairListUtil::max_bound
+    // J bra view per Hermite class
+    JBraClass jb[kNHerm];
+    // K-invert rows: [L_indexed][L_partner]
+    KInvClass kinv[kNL][kNL];
+    KInvData kdat;
+    bool kinv_built = false;
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = LSJK_PREC_MIXED;
+    DBuf<double> boys64, rys64;     // quadrature tables (FP64)
+    DBuf<float> boys32, rys32;      // FP32 copies for the mixed path
+    DBuf<double> rys_asym64;
+    DBuf<float> rys_asym32;
+    DBuf<int> status;               // kernel error word
+    DBuf<unsigned long long> counters;  // quartet counters and work queues
+    lsjk_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    // scratch buffers reused across calls (grown on demand)
+    std::vector<std::unique_ptr<DBuf<char>>> scratch;
+    size_t scratch_used = 0;
+    char* scratch_take(size_t bytes);
+    void scratch_reset() { scratch_used = 0; }
+    int smem_optin = 0;
+};
+
+// Stream-ordered scratch: a bump allocator over a few large blocks, reset at
+// the start of every build (all kernels of one build run on one stream).
+inline char* Context::scratch_take(size_t bytes)
+{
+    bytes = (bytes + 255) & ~size_t(255);
+    size_t used = 0;
+    for (auto& blk : scratch) {
+        if (scratch_used < used + blk->n) {
+            size_t off = scratch_used - used;
+            if (off + bytes <= blk->n) {
+                scratch_used += bytes;
+                return blk->p + off;
+            }
+            // skip the rest of this block
+            scratch_used = used + blk->n;
+        }
+        used += blk->n;
+    }
+    size_t sz = std::max(bytes, size_t(64) << 20);
+    scratch.emplace_back(new DBuf<char>());
+    scratch.back()->alloc(sz);
+    scratch_used = used + bytes;
+    return scratch.back()->p;
+}
+
+template <typename T>
+inline T* take(Context* ctx, size_t n) { return reinterpret_cast<T*>(ctx->scratch_take(sizeof(T) * (n ? n : 1))); }
+
+// Build steps (basis.cu, pairs.cu, jbuild.cu, kbuild.cu)
+void basis_init(Context* ctx, Basis* B);
+double j_quartet_flops(int LB, int LK);
+double k_quartet_flops(int L1, int L2, int L3, int L4);
+void build_pairlist(Context* ctx, PairList* pl);
+void build_kinv(Context* ctx, PairList* pl);
+void pure_to_cart(Context* ctx, const Basis* b1, const Basis* b2, const double* Dpure, double* Dcart);
+void cart_to_pure_acc(Context* ctx, const Basis* b1, const Basis* b2, const double* Xcart, double* Xpure);
+
+struct Ewald {
+    std::vector<double> alpha, omega;   // terms with alpha != 0 and omega != 0
+};
+
+void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
+                   const double* Dcart, double* Jcart, float thresp, float thredp);
+void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
+                    const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
+                    float thresp, float thredp);
+
+} // namespace lsjk

@@ -1,0 +1,184 @@
+// Python binding of the host API (module lightspeed_b200._lightspeed), with
+// the class and method names of the reference's Boost.Python module
+// (src/python/export_intbox.cpp:127-158, export_core.cpp:241-309,
+// export_env.cpp:19-66, export_tensor.cpp:8-24).
+#include <pybind11/pybind11.h>
+#include <pybind11/numpy.h>
+#include <pybind11/stl.h>
+#include "lightspeed.hpp"
+
+namespace py = pybind11;
+using namespace lightspeed;
+
+namespace {
+
+py::array tensor_view(const std::shared_ptr<Tensor>& t)
+{
+    std::vector<py::ssize_t> shape(t->shape().begin(), t->shape().end());
+    std::vector<py::ssize_t> strides(shape.size());
+    py::ssize_t s = sizeof(double);
+    for (int k = (int) shape.size() - 1; k >= 0; --k) {
+        strides[k] = s;
+        s *= shape[k];
+    }
+    // the numpy array keeps the Tensor alive through its base object
+    py::object owner = py::cast(t);
+    return py::array(py::dtype::of<double>(), shape, strides, t->data().data(), owner);
+}
+
+std::shared_ptr<Tensor> tensor_from_array(py::array_t<double, py::array::c_style | py::array::forcecast> a,
+                                          const std::string& name)
+{
+    std::vector<size_t> shape(a.shape(), a.shape() + a.ndim());
+    auto t = std::make_shared<Tensor>(shape, name);
+    std::copy(a.data(), a.data() + a.size(), t->data().begin());
+    return t;
+}
+
+py::dict stats_dict()
+{
+    lsjk_stats st{};
+    check_rc(lsjk_context_stats(Engine::instance().ctx(), &st), "stats");
+    py::dict d;
+    d["quartets_fp64"] = st.quartets_fp64;
+    d["quartets_fp32"] = st.quartets_fp32;
+    d["j_quartets"] = st.j_quartets;
+    d["k_quartets"] = st.k_quartets;
+    d["flops_j"] = st.flops_j;
+    d["flops_k"] = st.flops_k;
+    d["kernel_launches"] = st.kernel_launches;
+    return d;
+}
+
+} // namespace
+
+PYBIND11_MODULE(_lightspeed, m)
+{
+    m.doc() = "B200 J/K engine: host API mirroring the Lightspeed IntBox J/K path";
+
+    py::class_<Tensor, std::shared_ptr<Tensor>>(m, "Tensor", py::buffer_protocol())
+        .def(py::init<const std::vector<size_t>&, const std::string&>(), py::arg("shape"), py::arg("name") = "T")
+        .def_property_readonly("shape", [](const Tensor& t) { return py::tuple(py::cast(t.shape())); })
+        .def_property_readonly("ndim", &Tensor::ndim)
+        .def_property_readonly("size", &Tensor::size)
+        .def_property_readonly("name", &Tensor::name)
+        .def_property_readonly("np", [](const std::shared_ptr<Tensor>& t) { return tensor_view(t); })
+        .def("clone", &Tensor::clone)
+        .def("zero", &Tensor::zero)
+        .def("shape_error", &Tensor::shape_error)
+        .def("__str__", &Tensor::string)
+        .def_static("array", &tensor_from_array, py::arg("array"), py::arg("name") = "T")
+        .def_static("zeros", [](const std::vector<size_t>& shape, const std::string& name) {
+            return std::make_shared<Tensor>(shape, name);
+        }, py::arg("shape"), py::arg("name") = "T")
+        .def_buffer([](Tensor& t) -> py::buffer_info {
+            std::vector<py::ssize_t> shape(t.shape().begin(), t.shape().end());
+            std::vector<py::ssize_t> strides(shape.size());
+            py::ssize_t s = sizeof(double);
+            for (int k = (int) shape.size() - 1; k >= 0; --k) {
+                strides[k] = s;
+                s *= shape[k];
+            }
+            return py::buffer_info(t.data().data(), sizeof(double), py::format_descriptor<double>::format(),
+                                   (py::ssize_t) shape.size(), shape, strides);
+        });
+
+    py::class_<Primitive>(m, "Primitive")
+        .def(py::init<double, double, double, double, double, double, int, bool, int, int, int, int, int>(),
+             py::arg("c"), py::arg("e"), py::arg("x"), py::arg("y"), py::arg("z"), py::arg("c0"), py::arg("L"),
+             py::arg("is_pure"), py::arg("aoIdx"), py::arg("cartIdx"), py::arg("primIdx"), py::arg("shellIdx"),
+             py::arg("atomIdx"))
+        .def_property_readonly("c", &Primitive::c)
+        .def_property_readonly("e", &Primitive::e)
+        .def_property_readonly("x", &Primitive::x)
+        .def_property_readonly("y", &Primitive::y)
+        .def_property_readonly("z", &Primitive::z)
+        .def_property_readonly("c0", &Primitive::c0)
+        .def_property_readonly("L", &Primitive::L)
+        .def_property_readonly("is_pure", &Primitive::is_pure)
+        .def_property_readonly("aoIdx", &Primitive::aoIdx)
+        .def_property_readonly("cartIdx", &Primitive::cartIdx)
+        .def_property_readonly("primIdx", &Primitive::primIdx)
+        .def_property_readonly("shellIdx", &Primitive::shellIdx)
+        .def_property_readonly("atomIdx", &Primitive::atomIdx)
+        .def_property_readonly("ncart", &Primitive::ncart)
+        .def_property_readonly("npure", &Primitive::npure)
+        .def_property_readonly("nao", &Primitive::nao)
+        .def("__eq__", &Primitive::operator==);
+
+    py::class_<Basis, std::shared_ptr<Basis>>(m, "Basis")
+        .def(py::init<const std::string&, const std::vector<Primitive>&>(), py::arg("name"), py::arg("primitives"))
+        .def_property_readonly("name", &Basis::name)
+        .def_property_readonly("primitives", &Basis::primitives)
+        .def_property_readonly("nao", &Basis::nao)
+        .def_property_readonly("ncart", &Basis::ncart)
+        .def_property_readonly("nprim", &Basis::nprim)
+        .def_property_readonly("nshell", &Basis::nshell)
+        .def_property_readonly("natom", &Basis::natom)
+        .def_property_readonly("max_L", &Basis::max_L)
+        .def_property_readonly("has_pure", &Basis::has_pure)
+        .def_static("equivalent", &Basis::equivalent)
+        .def_static("concatenate", &Basis::concatenate)
+        .def("__str__", &Basis::string);
+
+    py::class_<Pair>(m, "Pair")
+        .def_property_readonly("prim1", &Pair::prim1, py::return_value_policy::reference_internal)
+        .def_property_readonly("prim2", &Pair::prim2, py::return_value_policy::reference_internal)
+        .def_property_readonly("bound", &Pair::bound);
+
+    py::class_<PairListL>(m, "PairListL")
+        .def_property_readonly("is_symmetric", &PairListL::is_symmetric)
+        .def_property_readonly("L1", &PairListL::L1)
+        .def_property_readonly("L2", &PairListL::L2)
+        .def_property_readonly("pairs", &PairListL::pairs, py::return_value_policy::reference_internal);
+
+    py::class_<PairList, std::shared_ptr<PairList>>(m, "PairList")
+        .def_static("build_schwarz", &PairList::build_schwarz, py::arg("basis1"), py::arg("basis2"),
+                    py::arg("is_symmetric"), py::arg("thre"))
+        .def_property_readonly("basis1", &PairList::basis1)
+        .def_property_readonly("basis2", &PairList::basis2)
+        .def_property_readonly("is_symmetric", &PairList::is_symmetric)
+        .def_property_readonly("thre", &PairList::thre)
+        .def_property_readonly("pairlists", &PairList::pairlists, py::return_value_policy::reference_internal)
+        .def("__str__", &PairList::string);
+
+    py::class_<Ewald, std::shared_ptr<Ewald>>(m, "Ewald")
+        .def(py::init<const std::vector<double>&, const std::vector<double>&>(), py::arg("scales"),
+             py::arg("omegas"))
+        .def_static("coulomb", &Ewald::coulomb)
+        .def_property_readonly("scales", &Ewald::scales)
+        .def_property_readonly("omegas", &Ewald::omegas)
+        .def_property_readonly("is_coulomb", &Ewald::is_coulomb);
+
+    py::class_<ResourceList, std::shared_ptr<ResourceList>>(m, "ResourceList")
+        .def_static("build", &ResourceList::build, py::arg("cpu_memory") = 1024, py::arg("gpu_memory") = 1024)
+        .def_static("build_cpu", &ResourceList::build_cpu)
+        .def_property_readonly("nthread", &ResourceList::nthread)
+        .def_property_readonly("ngpu", &ResourceList::ngpu)
+        .def("__str__", &ResourceList::string);
+
+    py::class_<IntBox>(m, "IntBox")
+        .def_static("coulomb", &IntBox::coulomb, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
+                    py::arg("pairlist34"), py::arg("D34"), py::arg("thresp"), py::arg("thredp"),
+                    py::arg("J12") = std::shared_ptr<Tensor>(), py::call_guard<py::gil_scoped_release>())
+        .def_static("exchange", &IntBox::exchange, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
+                    py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"), py::arg("thresp"),
+                    py::arg("thredp"), py::arg("K13") = std::shared_ptr<Tensor>(),
+                    py::call_guard<py::gil_scoped_release>())
+        .def_static("coulombMulti", &IntBox::coulombMulti, py::arg("resources"), py::arg("ewald"),
+                    py::arg("pairlist12"), py::arg("pairlist34"), py::arg("D34"), py::arg("thresp"),
+                    py::arg("thredp"), py::arg("J12") = std::vector<std::shared_ptr<Tensor>>(),
+                    py::call_guard<py::gil_scoped_release>())
+        .def_static("exchangeMulti", &IntBox::exchangeMulti, py::arg("resources"), py::arg("ewald"),
+                    py::arg("pairlist12"), py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"),
+                    py::arg("thresp"), py::arg("thredp"), py::arg("K13") = std::vector<std::shared_ptr<Tensor>>(),
+                    py::call_guard<py::gil_scoped_release>());
+
+    m.attr("PREC_MIXED") = LSJK_PREC_MIXED;
+    m.attr("PREC_FP64") = LSJK_PREC_FP64;
+    m.def("set_precision", [](int mode) { Engine::instance().set_precision(mode); });
+    m.def("get_precision", []() { return Engine::instance().precision(); });
+    m.def("stats", &stats_dict);
+    m.def("reset_stats", []() { check_rc(lsjk_context_reset_stats(Engine::instance().ctx()), "reset_stats"); });
+    m.def("engine_version", []() { return std::string(lsjk_version()); });
+}

@@ -1,0 +1,30 @@
+// Arguments of the J kernel and the declaration of its per-class launcher
+// (defined in jkernel.cuh, instantiated in jinst.cu).
+#pragma once
+#include "engine.cuh"
+
+namespace lsjk {
+
+constexpr int kJThreads = 128;   // bra pairs per CTA (one per thread)
+constexpr int kJChunk = 512;     // ket pairs per CTA
+
+struct JArgs {
+    const double* bgeom;      // bra: n x 4 (p, P)
+    const float* bbound;
+    const int* nbra;          // device count after truncation
+    double* jbra;             // n x HB accumulators
+    const double* krec;       // ket records (q, Q, D_u...)
+    const float* kbound;
+    const int* nket;
+    const double* boys;       // Boys table of order LB+LK
+    int* status;
+    unsigned long long* qcount;
+    int nterm;
+    double alpha[4], omega[4];
+    float thresp;
+};
+
+template <int LB, int LK>
+void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full);
+
+} // namespace lsjk

@@ -1,0 +1,387 @@
+// Coulomb (J) build on the device: the reference's coulombCPU pipeline
+// (src/cpp/intbox/cpu/coulomb.cpp:14-196) re-laid out for the B200.
+//
+//  1. ket screening: B34' = B34 * max|D_cart block| (truncate_ket,
+//     src/cpp/core/pair_list_util.cpp:60-123), kept if > thresp/max12, and a
+//     radix sort by B34' descending per Hermite class L3+L4;
+//  2. bra truncation: bound >= thresp/max34 (truncate_bra, :32-59) -- a
+//     binary search on the bound-sorted bra list, on the device;
+//  3. ket Hermite densities D_u = (-1)^|u| K_cd/q sum_cd E^cd_u D'_cd
+//     (cart_to_herm with phases, src/cpp/core/hermite.cpp:9-206);
+//  4. the J kernel per Hermite class pair (LB|LK): one thread per bra pair,
+//     ket pairs streamed in bound order by the whole CTA, quartets kept iff
+//     B12 * B34' >= thresp (coulomb.cpp:113-115), Boys table staged in shared
+//     memory by a bulk (TMA) copy, Hermite integrals + density contraction in
+//     registers, FP64 accumulation; no ERI is stored;
+//  5. bra Hermite -> Cartesian (herm_to_cart, hermite.cpp:207-411) with the
+//     symmetric-list double write and 1/2 on diagonal primitive pairs.
+#include <algorithm>
+#include <cub/device/device_radix_sort.cuh>
+#include "engine.cuh"
+#include "hermite.cuh"
+#include "jargs.cuh"
+#include "lsjk_device.cuh"
+
+namespace lsjk {
+
+namespace {
+
+constexpr double kTwoPi52 = 34.986836655249725693;   // 2 pi^(5/2)
+
+inline unsigned nblk(long n, int t) { return (unsigned) ((n + t - 1) / t); }
+
+// ---- 1. ket screening -------------------------------------------------------
+
+__global__ void k_ket_screen(const int* __restrict__ p1, const int* __restrict__ p2,
+                             const float* __restrict__ bound, int n, BasisView b3, BasisView b4,
+                             int symm, const double* __restrict__ Dc, float thre,
+                             unsigned* __restrict__ key, int* __restrict__ val,
+                             int* __restrict__ nkept, unsigned* __restrict__ maxbits)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int i = p1[k], j = p2[k];
+    int a1 = b3.cart[i], a2 = b4.cart[j];
+    int c1 = ncart_of(b3.L[i]), c2 = ncart_of(b4.L[j]);
+    int ld = b4.ncart;
+    double v = 0.0;
+    for (int x = 0; x < c1; ++x)
+        for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a1 + x) * ld + a2 + y]));
+    if (symm)
+        for (int x = 0; x < c1; ++x)
+            for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a2 + y) * ld + a1 + x]));
+    float B2 = (float) (v * (double) bound[k]);
+    bool keep = B2 > thre;
+    key[k] = keep ? ~__float_as_uint(B2) : 0xffffffffu;
+    val[k] = k;
+    if (keep) {
+        atomicAdd(nkept, 1);
+        atomicMax(maxbits, __float_as_uint(B2));
+    }
+}
+
+// thre_bra = thresp / max34 (float), then count bra pairs with bound >= thre_bra.
+__global__ void k_bra_count(const unsigned* __restrict__ maxbits, float thresp, int nclass,
+                            const float* const* __restrict__ bounds, const int* __restrict__ nfull,
+                            int* __restrict__ nbra)
+{
+    int c = threadIdx.x;
+    if (c >= nclass) return;
+    unsigned mb = 0;
+    for (int k = 0; k < kNHerm; ++k) mb = max(mb, maxbits[k]);
+    float max34 = __uint_as_float(mb);
+    float thre = (float) ((double) thresp / (double) max34);   // inf when max34 == 0
+    int n = nfull[c];
+    const float* b = bounds[c];
+    int lo = 0, hi = n;                 // first index with b < thre
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (b[mid] >= thre) lo = mid + 1; else hi = mid;
+    }
+    nbra[c] = lo;
+}
+
+// ---- 3. ket Hermite densities -------------------------------------------------
+
+template <int L3, int L4>
+__device__ void ket_record(int i, int j, BasisView b3, BasisView b4, bool symm, const double* __restrict__ Dc,
+                           const double* __restrict__ geom, double* __restrict__ rec)
+{
+    constexpr int N3 = ncart_of(L3), N4 = ncart_of(L4), H = nherm_of(L3 + L4);
+    const double q = geom[0];
+    const double Q[3] = {geom[1], geom[2], geom[3]};
+    const double A[3] = {b3.x[i], b3.y[i], b3.z[i]};
+    const double B[3] = {b4.x[j], b4.y[j], b4.z[j]};
+    double QA[3], QB[3];
+    double R2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        QA[d] = Q[d] - A[d];
+        QB[d] = Q[d] - B[d];
+        R2 += (A[d] - B[d]) * (A[d] - B[d]);
+    }
+    const double e1 = b3.e[i], e2 = b4.e[j];
+    const double Kab = b3.c[i] * b4.c[j] * exp(-e1 * e2 / q * R2);
+    ECoef<L3, L4> E;
+    build_E<L3, L4>(q, QA, QB, E);
+    const int a1 = b3.cart[i], a2 = b4.cart[j], ld = b4.ncart;
+    const double scale = (symm && i == j) ? 0.5 : 1.0;
+    double Dp[N3][N4];
+#pragma unroll
+    for (int x = 0; x < N3; ++x)
+#pragma unroll
+        for (int y = 0; y < N4; ++y) {
+            double v = Dc[(long) (a1 + x) * ld + a2 + y];
+            if (symm) v += Dc[(long) (a2 + y) * ld + a1 + x];
+            Dp[x][y] = v * scale;
+        }
+    const double pre = Kab / q;
+    rec[0] = q;
+    rec[1] = Q[0];
+    rec[2] = Q[1];
+    rec[3] = Q[2];
+#pragma unroll
+    for (int t = 0; t < H; ++t) {
+        const int tx = herm_tx(t), ty = herm_ty(t), tz = herm_tz(t);
+        double s = 0.0;
+#pragma unroll
+        for (int x = 0; x < N3; ++x)
+#pragma unroll
+            for (int y = 0; y < N4; ++y) {
+                s += E.v[0][cart_lx(L3, x)][cart_lx(L4, y)][tx] * E.v[1][cart_ly(L3, x)][cart_ly(L4, y)][ty] *
+                     E.v[2][cart_lz(L3, x)][cart_lz(L4, y)][tz] * Dp[x][y];
+            }
+        rec[4 + t] = ((tx + ty + tz) & 1 ? -pre : pre) * s;
+    }
+}
+
+template <int LK>
+__global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__ nkept,
+                           const int* __restrict__ p1, const int* __restrict__ p2,
+                           const float* __restrict__ bound, const double* __restrict__ geom,
+                           BasisView b3, BasisView b4, int symm, const double* __restrict__ Dc,
+                           double* __restrict__ rec, float* __restrict__ kbound)
+{
+    constexpr int S = 4 + nherm_of(LK);
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nkept) return;
+    int src = perm[k];
+    int i = p1[src], j = p2[src];
+    int L3 = b3.L[i], L4 = b4.L[j];
+    double* r = rec + (long) k * S;
+    const double* g = geom + 4L * src;
+    // L3 + L4 == LK
+    if (LK == 0) ket_record<0, 0>(i, j, b3, b4, symm, Dc, g, r);
+    else if (LK == 1) { if (L3 == 1) ket_record<1, 0>(i, j, b3, b4, symm, Dc, g, r); else ket_record<0, 1>(i, j, b3, b4, symm, Dc, g, r); }
+    else if (LK == 2) {
+        if (L3 == 2) ket_record<2, 0>(i, j, b3, b4, symm, Dc, g, r);
+        else if (L3 == 1) ket_record<1, 1>(i, j, b3, b4, symm, Dc, g, r);
+        else ket_record<0, 2>(i, j, b3, b4, symm, Dc, g, r);
+    } else if (LK == 3) { if (L3 == 2) ket_record<2, 1>(i, j, b3, b4, symm, Dc, g, r); else ket_record<1, 2>(i, j, b3, b4, symm, Dc, g, r); }
+    else ket_record<2, 2>(i, j, b3, b4, symm, Dc, g, r);
+    (void) L4;
+}
+
+// kbound of the sorted ket: recomputed from the sort keys
+__global__ void k_ket_bounds(const unsigned* __restrict__ keys_sorted, const int* __restrict__ nkept,
+                             float* __restrict__ kbound)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nkept) return;
+    kbound[k] = __uint_as_float(~keys_sorted[k]);
+}
+
+// ---- 5. bra Hermite -> Cartesian --------------------------------------------
+
+template <int L1, int L2>
+__device__ void bra_to_cart(int i, int j, BasisView b1, BasisView b2, bool symm, const double* __restrict__ geom,
+                            const double* __restrict__ jt, double* __restrict__ Jc)
+{
+    constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), H = nherm_of(L1 + L2);
+    const double p = geom[0];
+    const double P[3] = {geom[1], geom[2], geom[3]};
+    const double A[3] = {b1.x[i], b1.y[i], b1.z[i]};
+    const double B[3] = {b2.x[j], b2.y[j], b2.z[j]};
+    double PA[3], PB[3];
+    double R2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        PA[d] = P[d] - A[d];
+        PB[d] = P[d] - B[d];
+        R2 += (A[d] - B[d]) * (A[d] - B[d]);
+    }
+    const double e1 = b1.e[i], e2 = b2.e[j];
+    double pre = kTwoPi52 / p * b1.c[i] * b2.c[j] * exp(-e1 * e2 / p * R2);
+    if (symm && i == j) pre *= 0.5;
+    ECoef<L1, L2> E;
+    build_E<L1, L2>(p, PA, PB, E);
+    const int a1 = b1.cart[i], a2 = b2.cart[j], ld = b2.ncart;
+#pragma unroll
+    for (int x = 0; x < N1; ++x)
+#pragma unroll
+        for (int y = 0; y < N2; ++y) {
+            double s = 0.0;
+#pragma unroll
+            for (int t = 0; t < H; ++t)
+                s += E.v[0][cart_lx(L1, x)][cart_lx(L2, y)][herm_tx(t)] *
+                     E.v[1][cart_ly(L1, x)][cart_ly(L2, y)][herm_ty(t)] *
+                     E.v[2][cart_lz(L1, x)][cart_lz(L2, y)][herm_tz(t)] * jt[t];
+            s *= pre;
+            atomicAdd(&Jc[(long) (a1 + x) * ld + a2 + y], s);
+            if (symm) atomicAdd(&Jc[(long) (a2 + y) * ld + a1 + x], s);
+        }
+}
+
+template <int LB>
+__global__ void k_herm_to_cart(const int* __restrict__ nbra, const int* __restrict__ p1,
+                               const int* __restrict__ p2, const double* __restrict__ geom,
+                               BasisView b1, BasisView b2, int symm, const double* __restrict__ jbra,
+                               double* __restrict__ Jc)
+{
+    constexpr int H = nherm_of(LB);
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nbra) return;
+    int i = p1[k], j = p2[k];
+    int L1 = b1.L[i];
+    const double* g = geom + 4L * k;
+    const double* jt = jbra + (long) k * H;
+    if (LB == 0) bra_to_cart<0, 0>(i, j, b1, b2, symm, g, jt, Jc);
+    else if (LB == 1) { if (L1 == 1) bra_to_cart<1, 0>(i, j, b1, b2, symm, g, jt, Jc); else bra_to_cart<0, 1>(i, j, b1, b2, symm, g, jt, Jc); }
+    else if (LB == 2) {
+        if (L1 == 2) bra_to_cart<2, 0>(i, j, b1, b2, symm, g, jt, Jc);
+        else if (L1 == 1) bra_to_cart<1, 1>(i, j, b1, b2, symm, g, jt, Jc);
+        else bra_to_cart<0, 2>(i, j, b1, b2, symm, g, jt, Jc);
+    } else if (LB == 3) { if (L1 == 2) bra_to_cart<2, 1>(i, j, b1, b2, symm, g, jt, Jc); else bra_to_cart<1, 2>(i, j, b1, b2, symm, g, jt, Jc); }
+    else bra_to_cart<2, 2>(i, j, b1, b2, symm, g, jt, Jc);
+}
+
+template <int LB>
+void launch_j_row(Context* ctx, const JArgs& A, int LK, int nbra_full, int nket_full)
+{
+    switch (LK) {
+    case 0: launch_j<LB, 0>(ctx, A, nbra_full, nket_full); break;
+    case 1: launch_j<LB, 1>(ctx, A, nbra_full, nket_full); break;
+    case 2: launch_j<LB, 2>(ctx, A, nbra_full, nket_full); break;
+    case 3: launch_j<LB, 3>(ctx, A, nbra_full, nket_full); break;
+    case 4: launch_j<LB, 4>(ctx, A, nbra_full, nket_full); break;
+    }
+}
+
+} // namespace
+
+// Algorithmic FP64/FP32 flops of one J quartet of Hermite class (LB|LK):
+// prefactor/geometry 16, Boys (table 8 FMA + L recursion steps + exp),
+// Hermite recursion (one FMA per R^{(n)}_{tuv}) and the contraction (2 flops
+// per (t,u)); counted once per Ewald term.
+double j_quartet_flops(int LB, int LK)
+{
+    int L = LB + LK;
+    double nR = 0;
+    for (int n = 0; n <= L; ++n) nR += nherm_of(L - n);
+    return 16.0 + (16.0 + 3.0 * L + 1.0) + 2.0 * nR + 2.0 * nherm_of(LB) * nherm_of(LK);
+}
+
+void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
+                   const double* Dcart, double* Jcart, float thresp, float thredp)
+{
+    (void) thredp;
+    cudaStream_t s = ctx->stream;
+    const Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    // thresp / max12 (truncate_ket threshold), float as in the reference call
+    const float thre_ket = (float) ((double) thresp / pl12->max_bound);
+    int* counts = take<int>(ctx, 4 * kNHerm);          // nket[5], nbra[5]
+    unsigned* maxbits = take<unsigned>(ctx, kNHerm);
+    unsigned long long* qcnt = ctx->counters.p;   // FP64 J classes
+    LSJK_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * 4 * kNHerm, s));
+    LSJK_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * kNHerm, s));
+    int* nket = counts;
+    int* nbra = counts + kNHerm;
+    int* nfull = counts + 2 * kNHerm;
+    double* krec[kNHerm] = {};
+    float* kbound[kNHerm] = {};
+
+    // 1. ket screening + sort per Hermite class
+    for (int LK = 0; LK < kNHerm; ++LK) {
+        const JBraClass& jk = pl34->jb[LK];
+        int n = jk.n;
+        if (n == 0) continue;
+        unsigned* key = take<unsigned>(ctx, n);
+        unsigned* keys = take<unsigned>(ctx, n);
+        int* val = take<int>(ctx, n);
+        int* perm = take<int>(ctx, n);
+        k_ket_screen<<<nblk(n, 256), 256, 0, s>>>(jk.p1.p, jk.p2.p, jk.bound.p, n, b3->view(), b4->view(),
+                                                 pl34->symm ? 1 : 0, Dcart, thre_ket, key, val, nket + LK,
+                                                 maxbits + LK);
+        size_t tmp = 0;
+        LSJK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, keys, val, perm, n, 0, 32, s));
+        void* t = ctx->scratch_take(tmp);
+        LSJK_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, key, keys, val, perm, n, 0, 32, s));
+        krec[LK] = take<double>(ctx, (long) n * (4 + nherm_of(LK)));
+        kbound[LK] = take<float>(ctx, n);
+        k_ket_bounds<<<nblk(n, 256), 256, 0, s>>>(keys, nket + LK, kbound[LK]);
+        switch (LK) {
+        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        }
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches += 7;
+    }
+
+    // 2. bra truncation counts
+    {
+        const float* hb[kNHerm];
+        int hn[kNHerm];
+        for (int c = 0; c < kNHerm; ++c) {
+            hb[c] = pl12->jb[c].bound.p;
+            hn[c] = pl12->jb[c].n;
+        }
+        const float** db = take<const float*>(ctx, kNHerm);
+        LSJK_CUDA(cudaMemcpyAsync((void*) db, hb, sizeof(hb), cudaMemcpyHostToDevice, s));
+        LSJK_CUDA(cudaMemcpyAsync(nfull, hn, sizeof(hn), cudaMemcpyHostToDevice, s));
+        k_bra_count<<<1, 32, 0, s>>>(maxbits, thresp, kNHerm, db, nfull, nbra);
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    }
+
+    // 3./4. J kernels
+    double* jbra[kNHerm] = {};
+    for (int LB = 0; LB < kNHerm; ++LB) {
+        int n = pl12->jb[LB].n;
+        if (!n) continue;
+        jbra[LB] = take<double>(ctx, (long) n * nherm_of(LB));
+        LSJK_CUDA(cudaMemsetAsync(jbra[LB], 0, sizeof(double) * n * nherm_of(LB), s));
+    }
+    for (int LB = 0; LB < kNHerm; ++LB) {
+        const JBraClass& jb = pl12->jb[LB];
+        if (!jb.n) continue;
+        for (int LK = 0; LK < kNHerm; ++LK) {
+            const JBraClass& jk = pl34->jb[LK];
+            if (!jk.n) continue;
+            JArgs A{};
+            A.bgeom = jb.geom.p;
+            A.bbound = jb.bound.p;
+            A.nbra = nbra + LB;
+            A.jbra = jbra[LB];
+            A.krec = krec[LK];
+            A.kbound = kbound[LK];
+            A.nket = nket + LK;
+            A.boys = ctx->boys64.p + (long) (LB + LK) * LSJK_BOYS_NBIN * 8;
+            A.status = ctx->status.p;
+            A.qcount = qcnt + LB * kNHerm + LK;
+            A.nterm = (int) ew.alpha.size();
+            for (int t = 0; t < A.nterm; ++t) {
+                A.alpha[t] = ew.alpha[t];
+                A.omega[t] = ew.omega[t];
+            }
+            A.thresp = thresp;
+            switch (LB) {
+            case 0: launch_j_row<0>(ctx, A, LK, jb.n, jk.n); break;
+            case 1: launch_j_row<1>(ctx, A, LK, jb.n, jk.n); break;
+            case 2: launch_j_row<2>(ctx, A, LK, jb.n, jk.n); break;
+            case 3: launch_j_row<3>(ctx, A, LK, jb.n, jk.n); break;
+            case 4: launch_j_row<4>(ctx, A, LK, jb.n, jk.n); break;
+            }
+        }
+    }
+
+    // 5. back to Cartesian
+    for (int LB = 0; LB < kNHerm; ++LB) {
+        const JBraClass& jb = pl12->jb[LB];
+        if (!jb.n) continue;
+        unsigned g = nblk(jb.n, 128);
+        switch (LB) {
+        case 0: k_herm_to_cart<0><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+        case 1: k_herm_to_cart<1><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+        case 2: k_herm_to_cart<2><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+        case 3: k_herm_to_cart<3><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+        case 4: k_herm_to_cart<4><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+        }
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    }
+}
+
+} // namespace lsjk

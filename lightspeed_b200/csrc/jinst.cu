@@ -1,0 +1,15 @@
+// Instantiates the J kernels of one bra Hermite class (compiled once per
+// LSJK_LB = 0..4 by the build).
+#include "jkernel.cuh"
+
+#ifndef LSJK_LB
+#error "compile with -DLSJK_LB=<bra Hermite class>"
+#endif
+
+namespace lsjk {
+template void launch_j<LSJK_LB, 0>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 1>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 2>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 3>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 4>(Context*, const JArgs&, int, int);
+} // namespace lsjk

@@ -1,0 +1,279 @@
+// Exchange (K) build on the device: the reference's exchangeCPU
+// (src/cpp/intbox/cpu/exchange.cpp:17-355) re-laid out for the B200.
+//
+// The reference loops over (prim2, prim4) pairs -- rows of its K-invert lists
+// -- and inside over partners 1 of prim2 and 3 of prim4, both sorted by bound,
+// breaking as soon as bound12 * bound34 * max|D24 block| < thresp
+// (exchange.cpp:124-343). The computed quartet set is exactly
+//   { (1,2,3,4) : bound12 >= thre12, bound34 >= thre34,
+//                 double(float(bound12*bound34)) * Dmax(2,4) >= thresp },
+// with prim2 <= prim4 and the transposed write when D24 is symmetric.
+// Here:
+//  1. one device pass over all (prim2, prim4) pairs drops those whose first
+//     quartet already fails and appends the rest to per-class task lists;
+//  2. one kernel per class (L1 L2|L3 L4): each warp takes (prim2, prim4) tasks
+//     from a device work queue, keeps the D24 block in registers, walks the
+//     partner rows (prim1 uniform across the warp, prim3 across lanes), runs
+//     the Rys quadrature (tables staged in shared memory by a bulk copy) and
+//     contracts with D24 in registers, then scatters the K13 block with FP64
+//     atomics. No ERI is stored.
+#include <algorithm>
+#include "engine.cuh"
+#include "lsjk_device.cuh"
+#include "kargs.cuh"
+
+namespace lsjk {
+
+namespace {
+
+
+inline unsigned nblk(long n, int t) { return (unsigned) ((n + t - 1) / t); }
+
+__host__ __device__ inline int combo_index(int L1, int L2, int L3, int L4) { return ((L1 * kNL + L2) * kNL + L3) * kNL + L4; }
+constexpr int kNCombo = kNL * kNL * kNL * kNL;
+
+
+
+
+
+__global__ void k_absmax(const double* __restrict__ X, long n, unsigned long long* __restrict__ out)
+{
+    double m = 0.0;
+    for (long k = blockIdx.x * (long) blockDim.x + threadIdx.x; k < n; k += (long) gridDim.x * blockDim.x)
+        m = fmax(m, fabs(X[k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long) __double_as_longlong(m));
+}
+
+// thre12 = thresp / (max_bound(pl34) * D24max), thre34 likewise (exchange.cpp:54-71)
+__global__ void k_kscalars(KScalars* S, float thresp, double maxb12, double maxb34)
+{
+    double d = __longlong_as_double((long long) S->dmax_bits);
+    S->thre12 = (float) ((double) thresp / (maxb34 * d));
+    S->thre34 = (float) ((double) thresp / (maxb12 * d));
+}
+
+struct KRows {
+    const int* start[kNL][kNL];   // [L_indexed][L_partner]
+    const int* len[kNL][kNL];
+};
+
+struct TaskGenArgs {
+    BasisView b2, b4;
+    KRows r12, r34;
+    const float* pb12;
+    const float* pb34;
+    const double* Dc;
+    int ld4;
+    int d24symm;
+    float thresp;
+    const KScalars* sc;
+    KTask* tasks;                  // per-combo regions
+    const long* cap_off;           // region offsets
+    int* ntask;                    // per-combo counts
+};
+
+__global__ void k_task_gen(TaskGenArgs A)
+{
+    int i2 = blockIdx.y;
+    int i4 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i4 >= A.b4.nprim) return;
+    if (A.d24symm && i2 > i4) return;   // exchange.cpp:137-139
+    const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
+    int L2 = A.b2.L[i2], L4 = A.b4.L[i4];
+    int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
+    int n2 = ncart_of(L2), n4 = ncart_of(L4);
+    double dmax = 0.0;
+    for (int a = 0; a < n2; ++a)
+        for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[(long) (c2 + a) * A.ld4 + c4 + b]));
+    for (int L1 = 0; L1 < kNL; ++L1) {
+        const int* rl12 = A.r12.len[L2][L1];
+        if (!rl12) continue;
+        int len12 = rl12[i2];
+        if (!len12) continue;
+        float b12 = A.pb12[A.r12.start[L2][L1][i2]];
+        if (b12 < thre12) continue;
+        for (int L3 = 0; L3 < kNL; ++L3) {
+            const int* rl34 = A.r34.len[L4][L3];
+            if (!rl34) continue;
+            int len34 = rl34[i4];
+            if (!len34) continue;
+            float b34 = A.pb34[A.r34.start[L4][L3][i4]];
+            if (b34 < thre34) continue;
+            if ((double) (b12 * b34) * dmax < (double) A.thresp) continue;
+            int c = combo_index(L1, L2, L3, L4);
+            int slot = atomicAdd(&A.ntask[c], 1);
+            A.tasks[A.cap_off[c] + slot] = KTask{i2, i4, dmax};
+        }
+    }
+}
+
+
+
+// Runtime (L1,L2,L3,L4) -> template dispatch.
+template <int L1, int L2, int L3>
+void launch_k4(Context* ctx, const KArgs& A, long cap, int L4)
+{
+    switch (L4) {
+    case 0: launch_k<L1, L2, L3, 0>(ctx, A, cap); break;
+    case 1: launch_k<L1, L2, L3, 1>(ctx, A, cap); break;
+    case 2: launch_k<L1, L2, L3, 2>(ctx, A, cap); break;
+    }
+}
+template <int L1, int L2>
+void launch_k3(Context* ctx, const KArgs& A, long cap, int L3, int L4)
+{
+    switch (L3) {
+    case 0: launch_k4<L1, L2, 0>(ctx, A, cap, L4); break;
+    case 1: launch_k4<L1, L2, 1>(ctx, A, cap, L4); break;
+    case 2: launch_k4<L1, L2, 2>(ctx, A, cap, L4); break;
+    }
+}
+template <int L1>
+void launch_k2(Context* ctx, const KArgs& A, long cap, int L2, int L3, int L4)
+{
+    switch (L2) {
+    case 0: launch_k3<L1, 0>(ctx, A, cap, L3, L4); break;
+    case 1: launch_k3<L1, 1>(ctx, A, cap, L3, L4); break;
+    case 2: launch_k3<L1, 2>(ctx, A, cap, L3, L4); break;
+    }
+}
+void launch_k1(Context* ctx, const KArgs& A, long cap, int L1, int L2, int L3, int L4)
+{
+    switch (L1) {
+    case 0: launch_k2<0>(ctx, A, cap, L2, L3, L4); break;
+    case 1: launch_k2<1>(ctx, A, cap, L2, L3, L4); break;
+    case 2: launch_k2<2>(ctx, A, cap, L2, L3, L4); break;
+    }
+}
+
+} // namespace
+
+// Algorithmic flops of one K quartet of class (L1 L2|L3 L4) for one Ewald
+// term: geometry/prefactor 40, per root 16 (Rys tables) + 12 (recursion
+// coefficients) + 3 flops per 1-D integral entry over the three directions,
+// and 4 flops per (a,b,c,d) component product-and-contract.
+double k_quartet_flops(int L1, int L2, int L3, int L4)
+{
+    int nr = (L1 + L2 + L3 + L4) / 2 + 1;
+    double n1d = 3.0 * (L1 + L2 + 1) * (L3 + L4 + 1) + 3.0 * (L1 + 1) * (L2 + 1) * (L3 + 1) * (L4 + 1);
+    double nc = (double) ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4);
+    return 40.0 + nr * (28.0 + 2.0 * n1d + 4.0 * nc);
+}
+
+void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
+                    const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
+                    float thresp, float thredp)
+{
+    (void) thredp;
+    cudaStream_t s = ctx->stream;
+    const Basis *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    // global max |D24| (exchange.cpp:48-52) and the K-invert thresholds
+    KScalars* sc = take<KScalars>(ctx, 1);
+    LSJK_CUDA(cudaMemsetAsync(sc, 0, sizeof(KScalars), s));
+    long nd = (long) pl12->b2->ncart * b4->ncart;
+    if (nd) k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(Dcart, nd, &sc->dmax_bits);
+    k_kscalars<<<1, 1, 0, s>>>(sc, thresp, pl12->max_bound, pl34->max_bound);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 2;
+
+    // per-combo task regions: capacity = prims of L2 in basis2 x prims of L4 in basis4
+    int cnt2[kNL] = {0}, cnt4[kNL] = {0};
+    for (int L : b2->L) cnt2[L]++;
+    for (int L : b4->L) cnt4[L]++;
+    std::vector<long> off(kNCombo + 1, 0);
+    for (int L1 = 0; L1 < kNL; ++L1)
+        for (int L2 = 0; L2 < kNL; ++L2)
+            for (int L3 = 0; L3 < kNL; ++L3)
+                for (int L4 = 0; L4 < kNL; ++L4) {
+                    int c = combo_index(L1, L2, L3, L4);
+                    off[c + 1] = (long) cnt2[L2] * cnt4[L4];
+                }
+    for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
+    KTask* tasks = take<KTask>(ctx, off[kNCombo]);
+    long* doff = take<long>(ctx, kNCombo + 1);
+    int* ntask = take<int>(ctx, kNCombo);
+    unsigned* queue = take<unsigned>(ctx, kNCombo);
+    unsigned long long* qcnt = ctx->counters.p + kNJClass;   // FP64 K classes
+    LSJK_CUDA(cudaMemcpyAsync(doff, off.data(), sizeof(long) * (kNCombo + 1), cudaMemcpyHostToDevice, s));
+    LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
+    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * kNCombo, s));
+
+    TaskGenArgs G{};
+    G.b2 = b2->view();
+    G.b4 = b4->view();
+    for (int a = 0; a < kNL; ++a)
+        for (int b = 0; b < kNL; ++b) {
+            G.r12.start[a][b] = pl12->kinv[a][b].row_start.p;
+            G.r12.len[a][b] = pl12->kinv[a][b].row_len.p;
+            G.r34.start[a][b] = pl34->kinv[a][b].row_start.p;
+            G.r34.len[a][b] = pl34->kinv[a][b].row_len.p;
+        }
+    G.pb12 = pl12->kdat.pbound.p;
+    G.pb34 = pl34->kdat.pbound.p;
+    G.Dc = Dcart;
+    G.ld4 = b4->ncart;
+    G.d24symm = d24symm ? 1 : 0;
+    G.thresp = thresp;
+    G.sc = sc;
+    G.tasks = tasks;
+    G.cap_off = doff;
+    G.ntask = ntask;
+    if (b2->nprim && b4->nprim && pl12->kdat.nent && pl34->kdat.nent) {
+        dim3 grid(nblk(b4->nprim, 128), b2->nprim);
+        k_task_gen<<<grid, 128, 0, s>>>(G);
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    } else {
+        return;
+    }
+
+    for (int L1 = 0; L1 < kNL; ++L1)
+        for (int L2 = 0; L2 < kNL; ++L2)
+            for (int L3 = 0; L3 < kNL; ++L3)
+                for (int L4 = 0; L4 < kNL; ++L4) {
+                    int c = combo_index(L1, L2, L3, L4);
+                    long cap = off[c + 1] - off[c];
+                    if (!cap) continue;
+                    if (!pl12->kinv[L2][L1].row_len.p || !pl34->kinv[L4][L3].row_len.p) continue;
+                    int NR = (L1 + L2 + L3 + L4) / 2 + 1;
+                    KArgs A{};
+                    A.tasks = tasks + off[c];
+                    A.ntask = ntask + c;
+                    A.queue = queue + c;
+                    A.r12s = pl12->kinv[L2][L1].row_start.p;
+                    A.r12l = pl12->kinv[L2][L1].row_len.p;
+                    A.r34s = pl34->kinv[L4][L3].row_start.p;
+                    A.r34l = pl34->kinv[L4][L3].row_len.p;
+                    const KInvData& d12 = pl12->kdat;
+                    const KInvData& d34 = pl34->kdat;
+                    A.kab12 = d12.kab.p; A.e12 = d12.pe.p; A.x12 = d12.px.p; A.y12 = d12.py.p; A.z12 = d12.pz.p;
+                    A.cart12 = d12.pcart.p; A.b12 = d12.pbound.p;
+                    A.kab34 = d34.kab.p; A.e34 = d34.pe.p; A.x34 = d34.px.p; A.y34 = d34.py.p; A.z34 = d34.pz.p;
+                    A.cart34 = d34.pcart.p; A.b34 = d34.pbound.p;
+                    A.b2 = b2->view();
+                    A.b4 = b4->view();
+                    A.Dc = Dcart;
+                    A.ld4 = b4->ncart;
+                    A.Kc = Kcart;
+                    A.ld3 = b3->ncart;
+                    A.flip = flip_ok ? 1 : 0;
+                    A.thresp = thresp;
+                    A.sc = sc;
+                    A.rys = ctx->rys64.p + kRysOffset[NR];
+                    A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
+                    A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                    A.nbin = kRysNbin[NR];
+                    A.tmax = kRysTmax[NR];
+                    A.status = ctx->status.p;
+                    A.qcount = qcnt + c;
+                    A.nterm = (int) ew.alpha.size();
+                    for (int t = 0; t < A.nterm; ++t) {
+                        A.alpha[t] = ew.alpha[t];
+                        A.omega[t] = ew.omega[t];
+                    }
+                    launch_k1(ctx, A, cap, L1, L2, L3, L4);
+                }
+}
+
+} // namespace lsjk
