@@ -80,6 +80,9 @@ int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out);
 int lsjk_context_reset_stats(lsjk_context* ctx);
 /* Copy the device status word of the context's kernels (0 = no error). */
 int lsjk_context_status(lsjk_context* ctx, int* status);
+/* Measured FMA throughput of the device (fp64 = 1: FP64 pipe, 0: FP32),
+ * TFLOP/s; the roofline denominator of the J/K kernels. */
+int lsjk_measure_fma_peak(lsjk_context* ctx, int fp64, double* tflops);
 
 /* ---- basis: primitive shells exactly as lightspeed::Primitive
  * (src/lightspeed/basis.hpp:143-172); xyz is nprim x 3. Dense primIdx,
@@ -93,6 +96,13 @@ int lsjk_basis_create(lsjk_context* ctx, int nprim,
 int lsjk_basis_destroy(lsjk_basis* basis);
 int lsjk_basis_nao(const lsjk_basis* basis);
 int lsjk_basis_ncart(const lsjk_basis* basis);
+
+/* Cartesian -> pure coefficients of one shell of angular momentum L (0..6):
+ * coef is (2L+1) x ncart(L), pure order m = 0, +1, -1, +2, -2, ..., Cartesian
+ * order CCA lexical; the transform the engine applies to D, J and K (the
+ * reference's AngularMomentum coefficients, src/cpp/core/am.cpp:74-220).
+ * Host only; needs no GPU. */
+int lsjk_solid_harmonics(int L, double* coef);
 
 /* ---- pair list: PairList::build_schwarz (src/cpp/core/pair_list.cpp:29-177)
  * built on the device: Schwarz bounds of all primitive pairs (pair_list.cpp:

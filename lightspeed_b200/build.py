@@ -1,6 +1,8 @@
 """Build the native parts of lightspeed_b200 in-tree.
 
-  python -m lightspeed_b200.build [--jobs N] [--force]
+  python lightspeed_b200/build.py [--jobs N] [--force]
+
+(run as a script: the package itself imports the modules this builds)
 
 Steps (each skipped when its outputs are newer than its inputs):
   1. quadrature tables   tables/gen_tables.py   -> csrc/tables/quad_tables.inc
@@ -51,7 +53,7 @@ def gen_sources(force=False):
     inc = os.path.join(CSRC, "tables", "quad_tables.inc")
     gen = os.path.join(PKG, "tables", "gen_tables.py")
     if force or _mtime(inc) < _mtime(gen):
-        _run([sys.executable, "-m", "lightspeed_b200.tables.gen_tables"], cwd=ROOT)
+        _run([sys.executable, gen], cwd=ROOT)
     kgen = os.path.join(CSRC, "gen_kernels.py")
     jq = os.path.join(CSRC, "generated", "jquartets.cuh")
     if force or _mtime(jq) < _mtime(kgen):

@@ -1,4 +1,5 @@
 // extern "C" entry points of liblsjk.so (declared in include/lsjk.h).
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -11,6 +12,7 @@ struct lsjk_pairlist { lsjk::PairList p; };
 
 namespace lsjk {
 void basis_init(Context* ctx, Basis* B);
+std::vector<std::vector<double>> solid_harmonics(int L);
 }
 
 namespace {
@@ -113,9 +115,54 @@ void exchange_prepare(lsjk::Context* ctx, lsjk::PairList* pl12, lsjk::PairList* 
     if (pl34 != pl12) lsjk::build_kinv(ctx, pl34);
 }
 
+// FMA throughput probe: 8 independent dependency chains per thread so the
+// pipe, not latency, limits; every thread does 16 * iters flops.
+template <typename R>
+__global__ void k_fma_peak(R* out, int iters, R m, R c)
+{
+    R a0 = R(threadIdx.x) * R(1e-3), a1 = a0 + R(1), a2 = a0 + R(2), a3 = a0 + R(3);
+    R a4 = a0 + R(4), a5 = a0 + R(5), a6 = a0 + R(6), a7 = a0 + R(7);
+    for (int i = 0; i < iters; ++i) {
+        a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+        a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+    R s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == R(-12345.678)) out[threadIdx.x] = s;   // keeps the chains alive
+}
+
 } // namespace
 
 extern "C" {
+
+int lsjk_measure_fma_peak(lsjk_context* ctx, int fp64, double* tflops)
+{
+    return guard([&] {
+        if (!ctx || !tflops) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context& c = ctx->c;
+        set_device(c);
+        int nsm = 0;
+        LSJK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+        const int threads = 256, blocks = nsm * 8, iters = 1 << 14;
+        lsjk::DBuf<double> out;
+        out.alloc(threads);
+        float best = 1e30f;
+        for (int rep = 0; rep < 5; ++rep) {
+            LSJK_CUDA(cudaEventRecord(c.ev0, c.stream));
+            if (fp64)
+                k_fma_peak<double><<<blocks, threads, 0, c.stream>>>(out.p, iters, 0.999999, 1e-7);
+            else
+                k_fma_peak<float><<<blocks, threads, 0, c.stream>>>((float*) out.p, iters, 0.999999f, 1e-7f);
+            LSJK_CUDA(cudaGetLastError());
+            LSJK_CUDA(cudaEventRecord(c.ev1, c.stream));
+            LSJK_CUDA(cudaEventSynchronize(c.ev1));
+            float ms = 0.f;
+            LSJK_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+            if (rep > 0) best = std::min(best, ms);
+        }
+        double flops = 16.0 * iters * (double) threads * blocks;
+        *tflops = flops / (best * 1e-3) / 1e12;
+    });
+}
 
 const char* lsjk_last_error(void) { return g_err.c_str(); }
 
@@ -285,6 +332,17 @@ int lsjk_basis_destroy(lsjk_basis* basis)
 }
 
 int lsjk_basis_nao(const lsjk_basis* basis) { return basis ? basis->b.nao : -1; }
+
+int lsjk_solid_harmonics(int L, double* coef)
+{
+    return guard([&] {
+        if (L < 0 || L > 6 || !coef) throw lsjk::Error(LSJK_EINVAL, "solid_harmonics: L must be 0..6");
+        auto C = lsjk::solid_harmonics(L);
+        int nc = (L + 1) * (L + 2) / 2;
+        for (int p = 0; p < 2 * L + 1; ++p)
+            for (int k = 0; k < nc; ++k) coef[p * nc + k] = C[p][k];
+    });
+}
 int lsjk_basis_ncart(const lsjk_basis* basis) { return basis ? basis->b.ncart : -1; }
 
 int lsjk_pairlist_build_schwarz(lsjk_context* ctx, const lsjk_basis* basis1, const lsjk_basis* basis2,

@@ -6,6 +6,7 @@
 #include <pybind11/numpy.h>
 #include <pybind11/stl.h>
 #include "lightspeed.hpp"
+#include "oneint.hpp"
 
 namespace py = pybind11;
 using namespace lightspeed;
@@ -172,7 +173,21 @@ PYBIND11_MODULE(_lightspeed, m)
         .def_static("exchangeMulti", &IntBox::exchangeMulti, py::arg("resources"), py::arg("ewald"),
                     py::arg("pairlist12"), py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"),
                     py::arg("thresp"), py::arg("thredp"), py::arg("K13") = std::vector<std::shared_ptr<Tensor>>(),
-                    py::call_guard<py::gil_scoped_release>());
+                    py::call_guard<py::gil_scoped_release>())
+        // one-electron integrals for the SCF drivers (host C++)
+        .def_static("overlap", [](const std::shared_ptr<ResourceList>&, const std::shared_ptr<PairList>& pl,
+                                  const std::shared_ptr<Tensor>& S) { return OneInt::overlap(pl, S); },
+                    py::arg("resources"), py::arg("pairlist"), py::arg("S") = std::shared_ptr<Tensor>(),
+                    py::call_guard<py::gil_scoped_release>())
+        .def_static("kinetic", [](const std::shared_ptr<ResourceList>&, const std::shared_ptr<PairList>& pl,
+                                  const std::shared_ptr<Tensor>& T) { return OneInt::kinetic(pl, T); },
+                    py::arg("resources"), py::arg("pairlist"), py::arg("T") = std::shared_ptr<Tensor>(),
+                    py::call_guard<py::gil_scoped_release>())
+        .def_static("potential", [](const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ew,
+                                    const std::shared_ptr<PairList>& pl, const std::shared_ptr<Tensor>& xyzc,
+                                    const std::shared_ptr<Tensor>& V) { return OneInt::potential(ew, pl, xyzc, V); },
+                    py::arg("resources"), py::arg("ewald"), py::arg("pairlist"), py::arg("xyzc"),
+                    py::arg("V") = std::shared_ptr<Tensor>(), py::call_guard<py::gil_scoped_release>());
 
     m.attr("PREC_MIXED") = LSJK_PREC_MIXED;
     m.attr("PREC_FP64") = LSJK_PREC_FP64;
@@ -181,4 +196,43 @@ PYBIND11_MODULE(_lightspeed, m)
     m.def("stats", &stats_dict);
     m.def("reset_stats", []() { check_rc(lsjk_context_reset_stats(Engine::instance().ctx()), "reset_stats"); });
     m.def("engine_version", []() { return std::string(lsjk_version()); });
+    m.def("stream_handle", []() { return (uintptr_t) lsjk_context_stream(Engine::instance().ctx()); },
+          "cudaStream_t of the engine context, as an integer");
+    m.def("fma_peak_tflops", [](bool fp64) {
+        double t = 0.0;
+        check_rc(lsjk_measure_fma_peak(Engine::instance().ctx(), fp64 ? 1 : 0, &t), "fma_peak");
+        return t;
+    }, py::arg("fp64") = true);
+    // Device-resident J/K: D and J/K are device addresses (e.g. torch
+    // tensor.data_ptr()); the work is enqueued on the engine stream only.
+    m.def("coulomb_device", [](const std::shared_ptr<Ewald>& ew, const std::shared_ptr<PairList>& pl12,
+                               const std::shared_ptr<PairList>& pl34, const std::vector<uintptr_t>& D,
+                               const std::vector<uintptr_t>& J, float thresp, float thredp) {
+        if (D.size() != J.size()) throw std::runtime_error("coulomb_device: D/J count mismatch");
+        std::vector<const double*> dp;
+        std::vector<double*> jp;
+        for (size_t k = 0; k < D.size(); ++k) {
+            dp.push_back(reinterpret_cast<const double*>(D[k]));
+            jp.push_back(reinterpret_cast<double*>(J[k]));
+        }
+        check_rc(lsjk_coulomb_device(Engine::instance().ctx(), (int) ew->scales().size(), ew->scales().data(),
+                                     ew->omegas().data(), pl12->device_handle(), pl34->device_handle(),
+                                     (int) dp.size(), dp.data(), thresp, thredp, jp.data()),
+                 "coulomb_device");
+    }, py::call_guard<py::gil_scoped_release>());
+    m.def("exchange_device", [](const std::shared_ptr<Ewald>& ew, const std::shared_ptr<PairList>& pl12,
+                                const std::shared_ptr<PairList>& pl34, const std::vector<uintptr_t>& D,
+                                bool D24symm, const std::vector<uintptr_t>& K, float thresp, float thredp) {
+        if (D.size() != K.size()) throw std::runtime_error("exchange_device: D/K count mismatch");
+        std::vector<const double*> dp;
+        std::vector<double*> kp;
+        for (size_t k = 0; k < D.size(); ++k) {
+            dp.push_back(reinterpret_cast<const double*>(D[k]));
+            kp.push_back(reinterpret_cast<double*>(K[k]));
+        }
+        check_rc(lsjk_exchange_device(Engine::instance().ctx(), (int) ew->scales().size(), ew->scales().data(),
+                                      ew->omegas().data(), pl12->device_handle(), pl34->device_handle(),
+                                      (int) dp.size(), dp.data(), D24symm ? 1 : 0, thresp, thredp, kp.data()),
+                 "exchange_device");
+    }, py::call_guard<py::gil_scoped_release>());
 }

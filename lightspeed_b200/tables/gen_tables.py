@@ -22,7 +22,7 @@ x in [-1, 1] so the device can evaluate it with 8 fused multiply-adds (Horner).
 Interpolating ln w (then exponentiating) keeps small weights relatively
 accurate, as the reference's Rys tables also do (src/lightspeed/rys.hpp:109-153).
 
-Run:  python -m lightspeed_b200.tables.gen_tables   (takes ~1 minute)
+Run:  python lightspeed_b200/tables/gen_tables.py   (takes ~10 s)
 """
 import os
 import sys
