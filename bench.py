@@ -29,7 +29,7 @@ sys.path.insert(0, ROOT)
 METRIC = "J+K ms/iter & quartets/s: mixed vs FP64 GPU at |ΔE|≤1e-6 Eh; CPU ref alongside"
 THRE = 1.0e-14
 THREDP = 1.0e-5
-SAMPLE_CARBONS = 4        # CPU baseline sample: C4H10 / cc-pVDZ, full J+K
+SAMPLE_CARBONS = 8        # CPU baseline sample: C8H18 / cc-pVDZ, full J+K
 
 
 def parse():
@@ -40,7 +40,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--carbons", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--scf-maxiter", type=int, default=40)
+    ap.add_argument("--scf-maxiter", type=int, default=60)
+    ap.add_argument("--profile-step", action="store_true",
+                    help="after set-up and warm-up, run one FP64 J+K step between cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off) and exit")
     return ap.parse_args()
 
 
@@ -104,81 +107,74 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline(ls, nthread):
-    """Reference CPU IntBox (oracle/_ref) J+K on a bounded sample: C4H10 /
-    cc-pVDZ at the same thresholds, SCF-quality density from the GPU SCF;
-    quartets counted by the GPU engine on the same pair list and density."""
-    from oracle import ref
-    from lightspeed_b200.scf import RHF
-    if not ref.available():
-        return None
+def cpu_sample():
+    """Bounded CPU sample of the workload: C8H18 / cc-pVDZ (all-trans, same
+    thresholds) with its core-Hamiltonian density, built from the reference
+    CPU IntBox alone (S, T, V) so the reference arm runs no code of ours;
+    quartets are counted by the oracle's shared counting routine."""
+    import lightspeed_b200 as ls
+    from oracle import port, ref
     mol, bas = workload(ls, SAMPLE_CARBONS)
-    ls.set_precision(ls.PREC_FP64)
-    scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    scf.compute(maxiter=30, g_conv=1e-6)
-    D = scf.D
-    ls.reset_stats()
-    pl = scf.pairs
-    ew = ls.Ewald.coulomb()
-    res = ls.ResourceList.build()
-    ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), THRE, THRE)
-    ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, THRE, THRE)
-    nq = ls.stats()["j_quartets"] + ls.stats()["k_quartets"]
     rb = ref.RefBasis(ref.prim_arrays(bas))
     rp = ref.RefPairs(rb, rb, True, THRE)
+    S = ref.overlap(rp)
+    H = ref.kinetic(rp) + ref.potential(rp, mol.xyzZ)
+    s, U = np.linalg.eigh(S)
+    X = U / np.sqrt(s)
+    e, C = np.linalg.eigh(X.T @ H @ X)
+    nocc = int(round(mol.nuclear_charge)) // 2
+    Cocc = (X @ C)[:, :nocc]
+    D = Cocc @ Cocc.T
+    pb = port.Basis(bas.primitives)
+    ppl = port.Pairs(pb, pb, True, THRE)
+    nj, nk = port.count_quartets(ppl, ppl, D, D, True, THRE)
+    desc = ("C%dH%d/cc-pVDZ (%d bf) full J+K, FP64, thresp 1e-14, core-Hamiltonian density; "
+            "%.4g quartets per J+K" % (SAMPLE_CARBONS, 2 * SAMPLE_CARBONS + 2, bas.nao, nj + nk))
+    return rp, D, nj + nk, desc
+
+
+def time_reference(rp, D, nthread):
+    from oracle import ref
     t0 = time.time()
     ref.coulomb(rp, rp, D, THRE, THRE, nthread=nthread)
     ref.exchange(rp, rp, D, True, THRE, THRE, nthread=nthread)
-    dt = time.time() - t0
+    return time.time() - t0
+
+
+def cpu_baseline(nthread):
+    """The reference CPU IntBox (oracle/_ref) timed on the bounded sample."""
+    from oracle import port, ref
+    if not (ref.available() and port.available()):
+        return {"error": "oracle/_ref not built"}
+    rp, D, nq, desc = cpu_sample()
+    dt = time_reference(rp, D, nthread)
     return {"value": nq / dt, "unit": "quartets/s", "cores": nthread, "kind": "reference",
-            "sample": "C%dH%d/cc-pVDZ full J+K (%d bf), FP64, thresp 1e-14, converged RHF density; "
-                      "%.3g quartets in %.2f s" % (SAMPLE_CARBONS, 2 * SAMPLE_CARBONS + 2, bas.nao, nq, dt),
-            "seconds": dt}
+            "sample": desc + "; %.2f s" % dt, "seconds": dt}
 
 
 def run_reference(args):
     rank, world, local = dist_info()
     if rank != 0:
         return 0
-    import lightspeed_b200 as ls
-    from oracle import ref
-    if not ref.available():
+    from oracle import port, ref
+    if not (ref.available() and port.available()):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (reference CPU IntBox) is not built"}))
         return 0
     nthread = os.cpu_count() or 1
-    from lightspeed_b200.scf import RHF
-    mol, bas = workload(ls, SAMPLE_CARBONS)
-    ls.set_precision(ls.PREC_FP64)
-    scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    scf.compute(maxiter=30, g_conv=1e-6)
-    D = scf.D
-    ls.reset_stats()
-    res = ls.ResourceList.build()
-    ew = ls.Ewald.coulomb()
-    ls.IntBox.coulomb(res, ew, scf.pairs, scf.pairs, ls.Tensor.array(D), THRE, THRE)
-    ls.IntBox.exchange(res, ew, scf.pairs, scf.pairs, ls.Tensor.array(D), True, THRE, THRE)
-    nq = ls.stats()["j_quartets"] + ls.stats()["k_quartets"]
-    rb = ref.RefBasis(ref.prim_arrays(bas))
-    rp = ref.RefPairs(rb, rb, True, THRE)
+    rp, D, nq, desc = cpu_sample()
+    from oracle import ref as _r
     for _ in range(args.warmup):
-        ref.coulomb(rp, rp, D, THRE, THRE, nthread=nthread)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.time()
-        ref.coulomb(rp, rp, D, THRE, THRE, nthread=nthread)
-        ref.exchange(rp, rp, D, True, THRE, THRE, nthread=nthread)
-        times.append(time.time() - t0)
+        _r.coulomb(rp, rp, D, THRE, THRE, nthread=nthread)
+    times = [time_reference(rp, D, nthread) for _ in range(args.steps)]
     T = float(np.sum(times))
     v = nq * args.steps / T
-    sample = "C%dH%d/cc-pVDZ full J+K per step (%d bf), FP64, thresp 1e-14" % (SAMPLE_CARBONS,
-                                                                              2 * SAMPLE_CARBONS + 2, bas.nao)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "alkane J+K, sample of C40H82/cc-pVDZ", "sample": sample},
+        "config": {"workload": "C40H82/cc-pVDZ J+K, timed on a bounded sample", "sample": desc},
         "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": nthread, "kind": "reference",
-                         "sample": sample},
+                         "sample": desc},
         "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -200,7 +196,7 @@ def run_ours(args):
     ls.set_precision(ls.PREC_FP64)
     t0 = time.time()
     scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    E_scf = scf.compute(maxiter=args.scf_maxiter, g_conv=1e-6)
+    E_scf = scf.compute(maxiter=args.scf_maxiter, g_conv=1e-5)
     t_scf = time.time() - t0
     D = scf.D
     pl = scf.pairs
@@ -243,6 +239,19 @@ def run_ours(args):
         for _ in range(args.warmup):
             step(THREDP)
     torch.cuda.synchronize()
+    if args.profile_step:
+        ls.set_precision(ls.PREC_FP64)
+        torch.cuda.profiler.start()
+        step(THREDP)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        ls.set_precision(ls.PREC_MIXED)
+        torch.cuda.profiler.start()
+        step(THREDP)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_step": True, "workload": "C%dH%d/cc-pVDZ" % (args.carbons, 2 * args.carbons + 2)}))
+        return 0
     # quartet/flop counts of one step in each mode
     counts = {}
     for name, mode in (("fp64", ls.PREC_FP64), ("mixed", ls.PREC_MIXED)):
@@ -272,6 +281,7 @@ def run_ours(args):
     launches_fp64 = ls.stats()["kernel_launches"] - launches0
     msmx, mskmx = timed(ls.PREC_MIXED, THREDP, args.steps)
     torch.cuda.synchronize()
+    launches_timed = ls.stats()["kernel_launches"] - launches0
     # e2e through the public host API (H2D of D, D2H of J and K inside)
     Dt = ls.Tensor.array(D)
     e2e_ms = 0.0
@@ -321,7 +331,7 @@ def run_ours(args):
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(ls, os.cpu_count() or 1)
+            cpu = cpu_baseline(os.cpu_count() or 1)
         except Exception as ex:  # reported, never silently replaced
             cpu = {"error": str(ex)}
     line = {
@@ -354,7 +364,7 @@ def run_ours(args):
                      "fp32_peak": peak32},
         "e2e": {"value": e2e_qps, "unit": "quartets/s", "h2d_bytes_per_step": nao * nao * 8,
                 "d2h_bytes_per_step": 2 * nao * nao * 8, "ms_per_step": e2e_ms / args.steps},
-        "gpu_launches": int(launches_fp64),
+        "gpu_launches": int(launches_timed),
         "clocks": clk,
         "cpu_baseline": cpu,
     }

@@ -17,8 +17,13 @@ struct JArgs {
     const float* kbound;
     const int* nket;
     const double* boys;       // Boys table of order LB+LK
+    const float* krec32;      // FP32 copy of the ket records (mixed precision)
+    const float* boys32;      // FP32 Boys table of order LB+LK
     int* status;
-    unsigned long long* qcount;
+    unsigned long long* qcount;     // FP64 quartets of this class
+    unsigned long long* qcount32;   // FP32 quartets of this class
+    int mixed;                // 1: quartets with estimate < thredp run in FP32
+    float thredp;
     int nterm;
     double alpha[4], omega[4];
     float thresp;

@@ -140,7 +140,7 @@ __global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__
                            const int* __restrict__ p1, const int* __restrict__ p2,
                            const float* __restrict__ bound, const double* __restrict__ geom,
                            BasisView b3, BasisView b4, int symm, const double* __restrict__ Dc,
-                           double* __restrict__ rec, float* __restrict__ kbound)
+                           double* __restrict__ rec, float* __restrict__ rec32)
 {
     constexpr int S = 4 + nherm_of(LK);
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -160,6 +160,11 @@ __global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__
     } else if (LK == 3) { if (L3 == 2) ket_record<2, 1>(i, j, b3, b4, symm, Dc, g, r); else ket_record<1, 2>(i, j, b3, b4, symm, Dc, g, r); }
     else ket_record<2, 2>(i, j, b3, b4, symm, Dc, g, r);
     (void) L4;
+    if (rec32) {
+        float* r32 = rec32 + (long) k * S;
+#pragma unroll
+        for (int t = 0; t < S; ++t) r32[t] = (float) r[t];
+    }
 }
 
 // kbound of the sorted ket: recomputed from the sort keys
@@ -264,21 +269,23 @@ double j_quartet_flops(int LB, int LK)
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                    const double* Dcart, double* Jcart, float thresp, float thredp)
 {
-    (void) thredp;
     cudaStream_t s = ctx->stream;
     const Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
     // thresp / max12 (truncate_ket threshold), float as in the reference call
     const float thre_ket = (float) ((double) thresp / pl12->max_bound);
     int* counts = take<int>(ctx, 4 * kNHerm);          // nket[5], nbra[5]
     unsigned* maxbits = take<unsigned>(ctx, kNHerm);
-    unsigned long long* qcnt = ctx->counters.p;   // FP64 J classes
+    unsigned long long* qcnt = ctx->counters.p;                          // FP64 J classes
+    unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass;  // FP32 J classes
     LSJK_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * 4 * kNHerm, s));
     LSJK_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * kNHerm, s));
     int* nket = counts;
     int* nbra = counts + kNHerm;
     int* nfull = counts + 2 * kNHerm;
     double* krec[kNHerm] = {};
+    float* krec32[kNHerm] = {};
     float* kbound[kNHerm] = {};
+    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
 
     // 1. ket screening + sort per Hermite class
     for (int LK = 0; LK < kNHerm; ++LK) {
@@ -297,14 +304,15 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
         void* t = ctx->scratch_take(tmp);
         LSJK_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, key, keys, val, perm, n, 0, 32, s));
         krec[LK] = take<double>(ctx, (long) n * (4 + nherm_of(LK)));
+        if (mixed) krec32[LK] = take<float>(ctx, (long) n * (4 + nherm_of(LK)));
         kbound[LK] = take<float>(ctx, n);
         k_ket_bounds<<<nblk(n, 256), 256, 0, s>>>(keys, nket + LK, kbound[LK]);
         switch (LK) {
-        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
-        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
-        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
-        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
-        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], kbound[LK]); break;
+        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
+        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
+        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
+        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
+        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
         }
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches += 7;
@@ -351,6 +359,11 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             A.boys = ctx->boys64.p + (long) (LB + LK) * LSJK_BOYS_NBIN * 8;
             A.status = ctx->status.p;
             A.qcount = qcnt + LB * kNHerm + LK;
+            A.qcount32 = qcnt32 + LB * kNHerm + LK;
+            A.krec32 = krec32[LK];
+            A.boys32 = ctx->boys32.p + (long) (LB + LK) * LSJK_BOYS_NBIN * 8;
+            A.mixed = mixed ? 1 : 0;
+            A.thredp = thredp;
             A.nterm = (int) ew.alpha.size();
             for (int t = 0; t < A.nterm; ++t) {
                 A.alpha[t] = ew.alpha[t];

@@ -11,19 +11,96 @@ namespace lsjk {
 
 
 
+// One J quartet (bra pair in registers, ket record r) accumulated into jp.
+template <int LB, int LK>
+__device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, double p, double Px, double Py,
+                                            double Pz, const double* __restrict__ r, double* jp)
+{
+    constexpr int L = LB + LK;
+    const double q = r[0];
+    const double X = Px - r[1], Y = Py - r[2], Z = Pz - r[3];
+    const double R2 = X * X + Y * Y + Z * Z;
+    const double rs = rsqrt(p + q);
+    const double rho = p * q * (rs * rs);
+    for (int tm = 0; tm < A.nterm; ++tm) {
+        const double om = A.omega[tm];
+        double d2 = 1.0, f = A.alpha[tm] * rs;
+        if (om != -1.0) {
+            const double w2 = om * om;
+            d2 = w2 / (rho + w2);
+            f *= sqrt(d2);
+        }
+        const double rhoe = rho * d2;
+        double F[L + 1];
+        boys_eval<L, double>(rhoe * R2, tab, F);
+        double a[L + 1];
+        const double m2r = -2.0 * rhoe;
+        double pw = f;
+#pragma unroll
+        for (int n = 0; n <= L; ++n) {
+            a[n] = pw * F[n];
+            pw *= m2r;
+        }
+        jq_dispatch<LB, LK>(a, X, Y, Z, r + 4, jp);
+    }
+}
+
+// The same quartet in FP32 (geometry differences formed in FP64, everything
+// else in FP32), added to the FP64 accumulators.
+template <int LB, int LK>
+__device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, float p, double Px, double Py,
+                                            double Pz, const double* __restrict__ r, const float* __restrict__ r32,
+                                            double* jp)
+{
+    constexpr int L = LB + LK, HB = nherm_of(LB);
+    const float q = r32[0];
+    const float X = (float) (Px - r[1]), Y = (float) (Py - r[2]), Z = (float) (Pz - r[3]);
+    const float R2 = X * X + Y * Y + Z * Z;
+    const float rs = rsqrtf(p + q);
+    const float rho = p * q * (rs * rs);
+    float jq[HB];
+#pragma unroll
+    for (int t = 0; t < HB; ++t) jq[t] = 0.0f;
+    for (int tm = 0; tm < A.nterm; ++tm) {
+        const float om = (float) A.omega[tm];
+        float d2 = 1.0f, f = (float) A.alpha[tm] * rs;
+        if (A.omega[tm] != -1.0) {
+            const float w2 = om * om;
+            d2 = w2 / (rho + w2);
+            f *= sqrtf(d2);
+        }
+        const float rhoe = rho * d2;
+        float F[L + 1];
+        boys_eval<L, float>(rhoe * R2, tab, F);
+        float a[L + 1];
+        const float m2r = -2.0f * rhoe;
+        float pw = f;
+#pragma unroll
+        for (int n = 0; n <= L; ++n) {
+            a[n] = pw * F[n];
+            pw *= m2r;
+        }
+        jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4, jq);
+    }
+#pragma unroll
+    for (int t = 0; t < HB; ++t) jp[t] += (double) jq[t];
+}
+
 template <int LB, int LK>
 __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 {
-    constexpr int L = LB + LK, HB = nherm_of(LB), S = 4 + nherm_of(LK);
+    constexpr int HB = nherm_of(LB), S = 4 + nherm_of(LK);
     __shared__ __align__(128) double tab[LSJK_BOYS_NBIN * 8];
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(128) float tab32[LSJK_BOYS_NBIN * 8];
+    __shared__ __align__(8) uint64_t mbar[2];
     const int nb = *A.nbra, nk = *A.nket;
     const int i0 = blockIdx.x * kJThreads;
     const int j0 = blockIdx.y * kJChunk;
     if (i0 >= nb || j0 >= nk) return;
     const float B0 = A.bbound[i0];
     if (B0 * A.kbound[j0] < A.thresp) return;
-    if (!stage_bulk(tab, A.boys, sizeof(tab), &mbar, A.status)) return;
+    if (!stage_bulk(tab, A.boys, sizeof(tab), &mbar[0], A.status)) return;
+    if (A.mixed && !stage_bulk(tab32, A.boys32, sizeof(tab32), &mbar[1], A.status)) return;
 
     const int i = i0 + threadIdx.x;
     const bool act = i < nb;
@@ -36,42 +113,32 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         Pz = A.bgeom[4L * i + 3];
         Bi = A.bbound[i];
     }
+    const float p32 = (float) p;
+    const float thr_dp = A.mixed ? A.thredp : 0.0f;
     double jp[HB];
 #pragma unroll
     for (int t = 0; t < HB; ++t) jp[t] = 0.0;
-    long nq = 0;
+    long nq = 0, nq32 = 0;
     const int j1 = min(j0 + kJChunk, nk);
     for (int j = j0; j < j1; ++j) {
         const float Bj = A.kbound[j];
         if (B0 * Bj < A.thresp) break;
-        if (!act || Bi * Bj < A.thresp) continue;
-        ++nq;
+        const float est = Bi * Bj;
+        const bool pass = act && est >= A.thresp;
+        const bool dp = pass && est >= thr_dp;
+        const bool sp = pass && !dp;
         const double* r = A.krec + (long) j * S;
-        const double q = r[0];
-        const double X = Px - r[1], Y = Py - r[2], Z = Pz - r[3];
-        const double R2 = X * X + Y * Y + Z * Z;
-        const double rs = rsqrt(p + q);
-        const double rho = p * q * (rs * rs);
-        for (int tm = 0; tm < A.nterm; ++tm) {
-            const double om = A.omega[tm];
-            double d2 = 1.0, f = A.alpha[tm] * rs;
-            if (om != -1.0) {
-                const double w2 = om * om;
-                d2 = w2 / (rho + w2);
-                f *= sqrt(d2);
+        if (__any_sync(0xffffffffu, dp)) {
+            if (dp) {
+                ++nq;
+                j_quartet64<LB, LK>(A, tab, p, Px, Py, Pz, r, jp);
             }
-            const double rhoe = rho * d2;
-            double F[L + 1];
-            boys_eval<L, double>(rhoe * R2, tab, F);
-            double a[L + 1];
-            const double m2r = -2.0 * rhoe;
-            double pw = f;
-#pragma unroll
-            for (int n = 0; n <= L; ++n) {
-                a[n] = pw * F[n];
-                pw *= m2r;
+        }
+        if (__any_sync(0xffffffffu, sp)) {
+            if (sp) {
+                ++nq32;
+                j_quartet32<LB, LK>(A, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
             }
-            jq_dispatch<LB, LK>(a, X, Y, Z, r + 4, jp);
         }
     }
     if (act) {
@@ -79,11 +146,16 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         for (int t = 0; t < HB; ++t)
             if (jp[t] != 0.0) atomicAdd(&A.jbra[(long) i * HB + t], jp[t]);
     }
-    // quartet count for the statistics
-    for (int o = 16; o > 0; o >>= 1) nq += __shfl_xor_sync(0xffffffffu, nq, o);
-    if ((threadIdx.x & 31) == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
+    // quartet counts for the statistics
+    for (int o = 16; o > 0; o >>= 1) {
+        nq += __shfl_xor_sync(0xffffffffu, nq, o);
+        nq32 += __shfl_xor_sync(0xffffffffu, nq32, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nq) atomicAdd(A.qcount, (unsigned long long) nq);
+        if (nq32) atomicAdd(A.qcount32, (unsigned long long) nq32);
+    }
 }
-
 
 template <int LB, int LK>
 void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full)

@@ -48,7 +48,13 @@ struct KArgs {
     int nbin;
     double tmax;
     int* status;
-    unsigned long long* qcount;
+    unsigned long long* qcount;     // FP64 quartets of this class
+    unsigned long long* qcount32;   // FP32 quartets of this class
+    const float* rys32;             // FP32 copy of the table block
+    const float* asym_t32;
+    const float* asym_w32;
+    int mixed;                      // 1: estimate < thredp runs in FP32
+    float thredp;
     int nterm;
     double alpha[4], omega[4];
 };

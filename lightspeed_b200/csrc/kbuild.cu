@@ -165,7 +165,6 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
                     float thresp, float thredp)
 {
-    (void) thredp;
     cudaStream_t s = ctx->stream;
     const Basis *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
     // global max |D24| (exchange.cpp:48-52) and the K-invert thresholds
@@ -194,7 +193,9 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     long* doff = take<long>(ctx, kNCombo + 1);
     int* ntask = take<int>(ctx, kNCombo);
     unsigned* queue = take<unsigned>(ctx, kNCombo);
-    unsigned long long* qcnt = ctx->counters.p + kNJClass;   // FP64 K classes
+    unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
+    unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
+    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
     LSJK_CUDA(cudaMemcpyAsync(doff, off.data(), sizeof(long) * (kNCombo + 1), cudaMemcpyHostToDevice, s));
     LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
     LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * kNCombo, s));
@@ -267,6 +268,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.tmax = kRysTmax[NR];
                     A.status = ctx->status.p;
                     A.qcount = qcnt + c;
+                    A.qcount32 = qcnt32 + c;
+                    A.rys32 = ctx->rys32.p + kRysOffset[NR];
+                    A.asym_t32 = ctx->rys_asym32.p + NR * LSJK_RYS_NMAX;
+                    A.asym_w32 = ctx->rys_asym32.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                    A.mixed = mixed ? 1 : 0;
+                    A.thredp = thredp;
                     A.nterm = (int) ew.alpha.size();
                     for (int t = 0; t < A.nterm; ++t) {
                         A.alpha[t] = ew.alpha[t];

@@ -500,3 +500,122 @@ long port_pairs(const PBasis* b1, const PBasis* b2, int symm, float thre, int* p
         }
     return m;
 }
+
+/* ------------------------------------------------------- quartet counts */
+
+/* Number of primitive quartets the reference J and K evaluate for these pair
+ * lists, density (Cartesian) and thresholds -- the same screening as
+ * port_coulomb / port_exchange, without the integrals. Bra/ket loops use the
+ * bound ordering (binary search over the float-product condition, which is
+ * monotone), so this stays cheap at 1e5 pairs. */
+static int cmp_float_desc(const void* x, const void* y)
+{
+    float a = *(const float*) x, b = *(const float*) y;
+    return a > b ? -1 : (a < b);
+}
+
+/* count of leading entries v[k] (sorted desc) with (double)(float(b*v[k]))*s >= thr */
+static long count_prefix(const float* v, long n, float b, double s, float thr)
+{
+    long lo = 0, hi = n;
+    while (lo < hi) {
+        long mid = (lo + hi) / 2;
+        if ((double) (b * v[mid]) * s >= (double) thr) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+double port_count_j(const PBasis* b1, const PBasis* b2, long n12, const int* p12a, const int* p12b,
+                    const float* bnd12, int symm12, const PBasis* b3, const PBasis* b4, long n34,
+                    const int* p34a, const int* p34b, const float* bnd34, int symm34, const double* D34c,
+                    float thresp)
+{
+    (void) b1; (void) b2; (void) p12a; (void) p12b; (void) symm12;
+    const double max12 = max_bound(n12, bnd12);
+    const float thre_ket = (float) ((double) thresp / max12);
+    float* B34 = (float*) malloc(sizeof(float) * (n34 ? n34 : 1));
+    long nk = 0;
+    double max34 = 0.0;
+    const int ld4 = b4->ncart;
+    for (long k = 0; k < n34; ++k) {
+        int i = p34a[k], j = p34b[k];
+        int a1 = b3->cart[i], a2 = b4->cart[j], c1 = ncart_of(b3->L[i]), c2 = ncart_of(b4->L[j]);
+        double v = 0.0;
+        for (int x = 0; x < c1; ++x)
+            for (int y = 0; y < c2; ++y) {
+                double d = fabs(D34c[(long) (a1 + x) * ld4 + a2 + y]);
+                if (d > v) v = d;
+                if (symm34) {
+                    d = fabs(D34c[(long) (a2 + y) * ld4 + a1 + x]);
+                    if (d > v) v = d;
+                }
+            }
+        float B2 = (float) (v * (double) bnd34[k]);
+        if (B2 > thre_ket) {
+            B34[nk++] = B2;
+            if (B2 > max34) max34 = B2;
+        }
+    }
+    qsort(B34, nk, sizeof(float), cmp_float_desc);
+    const float thre_bra = (float) ((double) thresp / max34);
+    double total = 0.0;
+    for (long k = 0; k < n12; ++k) {
+        if (bnd12[k] < thre_bra) continue;
+        /* B12 * B34 >= thresp in float */
+        long lo = 0, hi = nk;
+        while (lo < hi) {
+            long mid = (lo + hi) / 2;
+            if (bnd12[k] * B34[mid] >= thresp) lo = mid + 1; else hi = mid;
+        }
+        total += (double) lo;
+    }
+    free(B34);
+    return total;
+}
+
+double port_count_k(const PBasis* b1, const PBasis* b2, long n12, const int* p12a, const int* p12b,
+                    const float* bnd12, int symm12, const PBasis* b3, const PBasis* b4, long n34,
+                    const int* p34a, const int* p34b, const float* bnd34, int symm34, const double* D24c,
+                    int d24symm, float thresp)
+{
+    (void) b1; (void) b3;
+    const long nD = (long) b2->ncart * b4->ncart;
+    double dmax = 0.0;
+    for (long k = 0; k < nD; ++k)
+        if (fabs(D24c[k]) > dmax) dmax = fabs(D24c[k]);
+    const float thre12 = (float) ((double) thresp / (max_bound(n34, bnd34) * dmax));
+    const float thre34 = (float) ((double) thresp / (max_bound(n12, bnd12) * dmax));
+    long m12, m34;
+    KEnt* e12 = kinv(n12, p12a, p12b, bnd12, symm12, thre12, &m12);
+    KEnt* e34 = kinv(n34, p34a, p34b, bnd34, symm34, thre34, &m34);
+    long* r12 = (long*) calloc(b2->nprim + 1, sizeof(long));
+    long* r34 = (long*) calloc(b4->nprim + 1, sizeof(long));
+    for (long k = 0; k < m12; ++k) r12[e12[k].idx + 1]++;
+    for (long k = 0; k < m34; ++k) r34[e34[k].idx + 1]++;
+    for (int k = 0; k < b2->nprim; ++k) r12[k + 1] += r12[k];
+    for (int k = 0; k < b4->nprim; ++k) r34[k + 1] += r34[k];
+    float* b34s = (float*) malloc(sizeof(float) * (m34 ? m34 : 1));
+    for (long k = 0; k < m34; ++k) b34s[k] = e34[k].b;
+    const int ld4 = b4->ncart;
+    double total = 0.0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (long t = 0; t < (long) b2->nprim * b4->nprim; ++t) {
+        int i2 = (int) (t / b4->nprim), i4 = (int) (t % b4->nprim);
+        if (d24symm && i2 > i4) continue;
+        int n2 = ncart_of(b2->L[i2]), n4 = ncart_of(b4->L[i4]);
+        int c2 = b2->cart[i2], c4 = b4->cart[i4];
+        double Dv = 0.0;
+        for (int a = 0; a < n2; ++a)
+            for (int b = 0; b < n4; ++b)
+                if (fabs(D24c[(long) (c2 + a) * ld4 + c4 + b]) > Dv) Dv = fabs(D24c[(long) (c2 + a) * ld4 + c4 + b]);
+        /* partners of each class are mixed in a row here: count per partner */
+        for (long k1 = r12[i2]; k1 < r12[i2 + 1]; ++k1) {
+            long n = 0;
+            for (long k3 = r34[i4]; k3 < r34[i4 + 1]; ++k3)
+                if ((double) (e12[k1].b * b34s[k3]) * Dv >= (double) thresp) ++n;
+            total += (double) n;
+        }
+    }
+    free(e12); free(e34); free(r12); free(r34); free(b34s);
+    return total;
+}

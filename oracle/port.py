@@ -162,3 +162,20 @@ def exchange(pl12, pl34, D, D24symm, thresp, scales=(1.0,), omegas=(-1.0,), equi
                         ctypes.c_long(len(pl34.pa)), _p(pl34.pa), _p(pl34.pb), _p(pl34.bound), int(pl34.symm), _p(Dc),
                         int(bool(D24symm) and eq13), len(s), _p(s), _p(o), ctypes.c_float(thresp), _p(Kc))
     return pl12.b1.T @ Kc @ pl34.b1.T.T
+
+
+def count_quartets(pl12, pl34, DJ, DK, DK_symm, thresp, equivalent13=None):
+    """(J quartets, K quartets) the reference evaluates for J with D34 = DJ
+    and K with D24 = DK (pure matrices) -- the shared counting routine that
+    turns a measured time into quartets/s for the CPU and the GPU alike."""
+    lib().port_count_j.restype = ctypes.c_double
+    lib().port_count_k.restype = ctypes.c_double
+    DJc = np.ascontiguousarray(pl34.b1.T.T @ DJ @ pl34.b2.T)
+    DKc = np.ascontiguousarray(pl12.b2.T.T @ DK @ pl34.b2.T)
+    eq13 = equivalent13 if equivalent13 is not None else (pl12.b1 is pl34.b1)
+    args = (ctypes.byref(pl12.b1.s), ctypes.byref(pl12.b2.s), ctypes.c_long(len(pl12.pa)), _p(pl12.pa),
+            _p(pl12.pb), _p(pl12.bound), int(pl12.symm), ctypes.byref(pl34.b1.s), ctypes.byref(pl34.b2.s),
+            ctypes.c_long(len(pl34.pa)), _p(pl34.pa), _p(pl34.pb), _p(pl34.bound), int(pl34.symm))
+    nj = lib().port_count_j(*args, _p(DJc), ctypes.c_float(thresp))
+    nk = lib().port_count_k(*args, _p(DKc), int(bool(DK_symm) and eq13), ctypes.c_float(thresp))
+    return nj, nk

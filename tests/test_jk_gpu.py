@@ -144,3 +144,25 @@ def test_shape_errors(ls, golden_dir):
     pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
     with pytest.raises(RuntimeError, match="shape"):
         ls.IntBox.coulomb(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.zeros((3, 3)), 1e-14, 1e-14)
+
+
+def test_quartet_sets_equal_reference(ls, golden_dir):
+    """The GPU evaluates exactly the reference's quartet set: its per-build
+    quartet counters equal the oracle's count of quartets passing the
+    reference screening (ket/bra truncation, K-invert thresholds, D24 symmetry)."""
+    from lightspeed_b200.geometry import water_cluster
+    from oracle import port
+    z = np.load(os.path.join(golden_dir, "oracle_w8.npz"))
+    bas = ls.Basis.from_gbs_file(water_cluster(8, seed=0), "6-31gs")
+    pb = port.Basis(bas.primitives)
+    ppl = port.Pairs(pb, pb, True, 1e-12)
+    for D, symm in ((z["D"], True), (z["D"] + 0.01 * np.tril(z["D"]), False)):
+        nj, nk = port.count_quartets(ppl, ppl, D, D, symm, 1e-12)
+        res = ls.ResourceList.build()
+        pl = ls.PairList.build_schwarz(bas, bas, True, 1e-12)
+        ls.reset_stats()
+        ls.IntBox.coulomb(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.array(D), 1e-12, 1e-12)
+        ls.IntBox.exchange(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.array(D), symm, 1e-12, 1e-12)
+        st = ls.stats()
+        assert st["j_quartets"] == nj
+        assert st["k_quartets"] == nk
