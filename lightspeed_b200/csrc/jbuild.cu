@@ -60,19 +60,25 @@ __global__ void k_ket_screen(const int* __restrict__ p1, const int* __restrict__
     }
 }
 
+// Bra class tables passed by value (no host->device copy, so a build can be
+// captured in a CUDA graph).
+struct BraTables {
+    const float* bound[kNHerm];
+    int n[kNHerm];
+};
+
 // thre_bra = thresp / max34 (float), then count bra pairs with bound >= thre_bra.
-__global__ void k_bra_count(const unsigned* __restrict__ maxbits, float thresp, int nclass,
-                            const float* const* __restrict__ bounds, const int* __restrict__ nfull,
+__global__ void k_bra_count(const unsigned* __restrict__ maxbits, float thresp, BraTables T,
                             int* __restrict__ nbra)
 {
     int c = threadIdx.x;
-    if (c >= nclass) return;
+    if (c >= kNHerm) return;
     unsigned mb = 0;
     for (int k = 0; k < kNHerm; ++k) mb = max(mb, maxbits[k]);
     float max34 = __uint_as_float(mb);
     float thre = (float) ((double) thresp / (double) max34);   // inf when max34 == 0
-    int n = nfull[c];
-    const float* b = bounds[c];
+    int n = T.n[c];
+    const float* b = T.bound[c];
     int lo = 0, hi = n;                 // first index with b < thre
     while (lo < hi) {
         int mid = (lo + hi) >> 1;
@@ -281,7 +287,6 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
     LSJK_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * kNHerm, s));
     int* nket = counts;
     int* nbra = counts + kNHerm;
-    int* nfull = counts + 2 * kNHerm;
     double* krec[kNHerm] = {};
     float* krec32[kNHerm] = {};
     float* kbound[kNHerm] = {};
@@ -320,16 +325,12 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
 
     // 2. bra truncation counts
     {
-        const float* hb[kNHerm];
-        int hn[kNHerm];
+        BraTables T{};
         for (int c = 0; c < kNHerm; ++c) {
-            hb[c] = pl12->jb[c].bound.p;
-            hn[c] = pl12->jb[c].n;
+            T.bound[c] = pl12->jb[c].bound.p;
+            T.n[c] = pl12->jb[c].n;
         }
-        const float** db = take<const float*>(ctx, kNHerm);
-        LSJK_CUDA(cudaMemcpyAsync((void*) db, hb, sizeof(hb), cudaMemcpyHostToDevice, s));
-        LSJK_CUDA(cudaMemcpyAsync(nfull, hn, sizeof(hn), cudaMemcpyHostToDevice, s));
-        k_bra_count<<<1, 32, 0, s>>>(maxbits, thresp, kNHerm, db, nfull, nbra);
+        k_bra_count<<<1, 32, 0, s>>>(maxbits, thresp, T, nbra);
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches++;
     }

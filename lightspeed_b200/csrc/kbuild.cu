@@ -69,7 +69,7 @@ struct TaskGenArgs {
     float thresp;
     const KScalars* sc;
     KTask* tasks;                  // per-combo regions
-    const long* cap_off;           // region offsets
+    long cap_off[kNCombo];         // region offsets (by value: graph-capturable)
     int* ntask;                    // per-combo counts
 };
 
@@ -190,13 +190,11 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                 }
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
-    long* doff = take<long>(ctx, kNCombo + 1);
     int* ntask = take<int>(ctx, kNCombo);
     unsigned* queue = take<unsigned>(ctx, kNCombo);
     unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
     unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
     const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
-    LSJK_CUDA(cudaMemcpyAsync(doff, off.data(), sizeof(long) * (kNCombo + 1), cudaMemcpyHostToDevice, s));
     LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
     LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * kNCombo, s));
 
@@ -218,7 +216,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     G.thresp = thresp;
     G.sc = sc;
     G.tasks = tasks;
-    G.cap_off = doff;
+    for (int c = 0; c < kNCombo; ++c) G.cap_off[c] = off[c];
     G.ntask = ntask;
     if (b2->nprim && b4->nprim && pl12->kdat.nent && pl34->kdat.nent) {
         dim3 grid(nblk(b4->nprim, 128), b2->nprim);
