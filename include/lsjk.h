@@ -78,6 +78,19 @@ int lsjk_context_set_precision(lsjk_context* ctx, int mode);
 void* lsjk_context_stream(lsjk_context* ctx);
 int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out);
 int lsjk_context_reset_stats(lsjk_context* ctx);
+/* Raw per-class quartet counters: [precision FP64, FP32][J classes (LB*5+LK),
+ * K classes ((L1*3+L2)*3+L3)*3+L4]; n must be >= 2*(25+81). */
+int lsjk_context_counters(lsjk_context* ctx, unsigned long long* out, int n);
+
+/* Autotuner. While on, every J/K build first times candidate launch schedules
+ * of each class it meets (J: ket pairs per CTA; K: CTAs per SM of each pass)
+ * on scratch outputs and keeps the fastest in the context's table; builds
+ * then use the table. The table (LSJK_TUNE_INTS ints: J chunk per (LB,LK),
+ * then K CTAs/SM per pass and class; 0 = default) can be saved and restored
+ * (set = 0: read, 1: write) so a workload is tuned once. */
+#define LSJK_TUNE_INTS (25 + 2 * 81)
+int lsjk_context_set_autotune(lsjk_context* ctx, int on);
+int lsjk_context_tune_table(lsjk_context* ctx, int* table, int n, int set);
 /* Copy the device status word of the context's kernels (0 = no error). */
 int lsjk_context_status(lsjk_context* ctx, int* status);
 /* Measured FMA throughput of the device (fp64 = 1: FP64 pipe, 0: FP32),
@@ -147,6 +160,19 @@ int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, con
                          const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
                          const double* const* D24_dev, int D24symm, float thresp, float thredp,
                          double* const* K13_dev);
+
+/* ---- CUDA graphs: capture the builds issued through the *_device entry
+ * points between lsjk_graph_begin and lsjk_graph_end on the context stream,
+ * then replay them with one lsjk_graph_launch (an SCF iteration's J+K as one
+ * graph). Each captured call must have run once before with the same pair
+ * lists, densities and sizes (one-time set-up and scratch growth happen
+ * outside capture). No reference counterpart: the reference re-enters
+ * TeraChem per call (tc/coulomb.cpp:30-55). */
+typedef struct lsjk_graph lsjk_graph;
+int lsjk_graph_begin(lsjk_context* ctx);
+int lsjk_graph_end(lsjk_context* ctx, lsjk_graph** out);
+int lsjk_graph_launch(lsjk_graph* graph);
+int lsjk_graph_destroy(lsjk_graph* graph);
 
 #ifdef __cplusplus
 }

@@ -9,6 +9,11 @@
 struct lsjk_context { lsjk::Context c; };
 struct lsjk_basis { lsjk::Basis b; };
 struct lsjk_pairlist { lsjk::PairList p; };
+struct lsjk_graph {
+    lsjk::Context* ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
 
 namespace lsjk {
 void basis_init(Context* ctx, Basis* B);
@@ -68,19 +73,25 @@ void check_lmax(const lsjk::PairList* pl)
         throw lsjk::Error(LSJK_ENOTSUPP, "J/K: angular momentum above d is not supported by the GPU kernels");
 }
 
-// One J or K build for one density, device pointers in and out.
-void coulomb_one(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
-                 const lsjk::PairList* pl34, const double* Dpure, double* Jpure, float thresp, float thredp)
+// One J build for ng (1..4) densities that share the quartet loop, device
+// pointers in and out.
+void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
+                   const lsjk::PairList* pl34, const double* const* Dpure, double* const* Jpure, int ng,
+                   float thresp, float thredp)
 {
     ctx->scratch_reset();
     const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
-    double* Dc = lsjk::take<double>(ctx, (size_t) b3->ncart * b4->ncart);
-    double* Jc = lsjk::take<double>(ctx, (size_t) b1->ncart * b2->ncart);
-    lsjk::pure_to_cart(ctx, b3, b4, Dpure, Dc);
-    LSJK_CUDA(cudaMemsetAsync(Jc, 0, sizeof(double) * b1->ncart * b2->ncart, ctx->stream));
+    double* Dc[lsjk::kJBatchMax];
+    double* Jc[lsjk::kJBatchMax];
+    for (int g = 0; g < ng; ++g) {
+        Dc[g] = lsjk::take<double>(ctx, (size_t) b3->ncart * b4->ncart);
+        Jc[g] = lsjk::take<double>(ctx, (size_t) b1->ncart * b2->ncart);
+        lsjk::pure_to_cart(ctx, b3, b4, Dpure[g], Dc[g]);
+        LSJK_CUDA(cudaMemsetAsync(Jc[g], 0, sizeof(double) * b1->ncart * b2->ncart, ctx->stream));
+    }
     if (!ew.alpha.empty() && pl12->npair && pl34->npair)
-        lsjk::coulomb_build(ctx, ew, pl12, pl34, Dc, Jc, thresp, thredp);
-    lsjk::cart_to_pure_acc(ctx, b1, b2, Jc, Jpure);
+        lsjk::coulomb_build(ctx, ew, pl12, pl34, Dc, Jc, ng, thresp, thredp);
+    for (int g = 0; g < ng; ++g) lsjk::cart_to_pure_acc(ctx, b1, b2, Jc[g], Jpure[g]);
 }
 
 void exchange_one(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
@@ -178,6 +189,7 @@ int lsjk_context_create(int device, lsjk_context** out)
             c.device = device;
             LSJK_CUDA(cudaSetDevice(device));
             LSJK_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            LSJK_CUDA(cudaDeviceGetAttribute(&c.nsm, cudaDevAttrMultiProcessorCount, device));
             std::vector<double> boys(kBoysCoef, kBoysCoef + sizeof(kBoysCoef) / sizeof(double));
             std::vector<double> rys(kRysCoef, kRysCoef + sizeof(kRysCoef) / sizeof(double));
             std::vector<double> asym(kRysAsymT, kRysAsymT + sizeof(kRysAsymT) / sizeof(double));
@@ -191,6 +203,7 @@ int lsjk_context_create(int device, lsjk_context** out)
             c.status.alloc(1);
             LSJK_CUDA(cudaMemsetAsync(c.status.p, 0, sizeof(int), c.stream));
             c.counters.alloc(lsjk::kNCounters);
+            c.tune_sink.alloc(lsjk::kNCounters);
             LSJK_CUDA(cudaMemsetAsync(c.counters.p, 0, sizeof(unsigned long long) * lsjk::kNCounters, c.stream));
             LSJK_CUDA(cudaEventCreate(&c.ev0));
             LSJK_CUDA(cudaEventCreate(&c.ev1));
@@ -263,6 +276,38 @@ int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out)
                         }
         }
         *out = st;
+    });
+}
+
+int lsjk_context_counters(lsjk_context* ctx, unsigned long long* out, int n)
+{
+    return guard([&] {
+        if (!ctx || !out || n < lsjk::kNCounters) throw lsjk::Error(LSJK_EINVAL, "bad counters buffer");
+        set_device(ctx->c);
+        LSJK_CUDA(cudaMemcpyAsync(out, ctx->c.counters.p, sizeof(unsigned long long) * lsjk::kNCounters,
+                                  cudaMemcpyDeviceToHost, ctx->c.stream));
+        LSJK_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+
+int lsjk_context_set_autotune(lsjk_context* ctx, int on)
+{
+    return guard([&] {
+        if (!ctx) throw lsjk::Error(LSJK_EINVAL, "null context");
+        ctx->c.tuning = on != 0;
+    });
+}
+
+int lsjk_context_tune_table(lsjk_context* ctx, int* table, int n, int set)
+{
+    return guard([&] {
+        if (!ctx || !table || n < lsjk::kTuneInts) throw lsjk::Error(LSJK_EINVAL, "bad tune table");
+        int* t = reinterpret_cast<int*>(&ctx->c.tune);
+        static_assert(sizeof(lsjk::Tune) == sizeof(int) * lsjk::kTuneInts, "Tune layout");
+        if (set)
+            std::copy(table, table + lsjk::kTuneInts, t);
+        else
+            std::copy(t, t + lsjk::kTuneInts, table);
     });
 }
 
@@ -407,8 +452,9 @@ int lsjk_coulomb_device(lsjk_context* ctx, int nterm, const double* scales, cons
         lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
         check_lmax(&pl12->p);
         check_lmax(&pl34->p);
-        for (int k = 0; k < ndens; ++k)
-            coulomb_one(&ctx->c, ew, &pl12->p, &pl34->p, D34[k], J12[k], thresp, thredp);
+        for (int k0 = 0; k0 < ndens; k0 += lsjk::kJBatchMax)
+            coulomb_group(&ctx->c, ew, &pl12->p, &pl34->p, D34 + k0, J12 + k0,
+                          std::min(lsjk::kJBatchMax, ndens - k0), thresp, thredp);
     });
 }
 
@@ -444,17 +490,28 @@ int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const doubl
         check_lmax(&pl34->p);
         const size_t nD = (size_t) pl34->p.b1->nao * pl34->p.b2->nao;
         const size_t nJ = (size_t) pl12->p.b1->nao * pl12->p.b2->nao;
+        const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
         lsjk::DBuf<double> dD, dJ;
-        dD.alloc(nD);
-        dJ.alloc(nJ);
-        std::vector<double> hJ(nJ);
-        for (int k = 0; k < ndens; ++k) {
-            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p, D34[k], sizeof(double) * nD, cudaMemcpyHostToDevice, c->stream));
-            if (nJ) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * nJ, c->stream));
-            coulomb_one(c, ew, &pl12->p, &pl34->p, dD.p, dJ.p, thresp, thredp);
-            if (nJ) LSJK_CUDA(cudaMemcpyAsync(hJ.data(), dJ.p, sizeof(double) * nJ, cudaMemcpyDeviceToHost, c->stream));
+        dD.alloc(nD * G);
+        dJ.alloc(nJ * G);
+        std::vector<double> hJ(nJ * G);
+        for (int k0 = 0; k0 < ndens; k0 += G) {
+            const int ng = std::min(G, ndens - k0);
+            const double* dp[lsjk::kJBatchMax];
+            double* jp[lsjk::kJBatchMax];
+            for (int g = 0; g < ng; ++g) {
+                dp[g] = dD.p + g * nD;
+                jp[g] = dJ.p + g * nJ;
+                if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p + g * nD, D34[k0 + g], sizeof(double) * nD,
+                                                  cudaMemcpyHostToDevice, c->stream));
+            }
+            if (nJ) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * nJ * ng, c->stream));
+            coulomb_group(c, ew, &pl12->p, &pl34->p, dp, jp, ng, thresp, thredp);
+            if (nJ) LSJK_CUDA(cudaMemcpyAsync(hJ.data(), dJ.p, sizeof(double) * nJ * ng, cudaMemcpyDeviceToHost,
+                                              c->stream));
             check_kernels(c);
-            for (size_t i = 0; i < nJ; ++i) J12[k][i] += hJ[i];
+            for (int g = 0; g < ng; ++g)
+                for (size_t i = 0; i < nJ; ++i) J12[k0 + g][i] += hJ[g * nJ + i];
         }
     });
 }
@@ -486,6 +543,56 @@ int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const doub
             check_kernels(c);
             for (size_t i = 0; i < nK; ++i) K13[k][i] += hK[i];
         }
+    });
+}
+
+int lsjk_graph_begin(lsjk_context* ctx)
+{
+    return guard([&] {
+        if (!ctx) throw lsjk::Error(LSJK_EINVAL, "null context");
+        set_device(ctx->c);
+        LSJK_CUDA(cudaStreamBeginCapture(ctx->c.stream, cudaStreamCaptureModeThreadLocal));
+    });
+}
+
+int lsjk_graph_end(lsjk_context* ctx, lsjk_graph** out)
+{
+    return guard([&] {
+        if (!ctx || !out) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        set_device(ctx->c);
+        auto* g = new lsjk_graph();
+        g->ctx = &ctx->c;
+        cudaError_t e = cudaStreamEndCapture(ctx->c.stream, &g->graph);
+        if (e != cudaSuccess) {
+            delete g;
+            throw lsjk::Error(LSJK_ECUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+        }
+        e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g->graph);
+            delete g;
+            throw lsjk::Error(LSJK_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+        }
+        *out = g;
+    });
+}
+
+int lsjk_graph_launch(lsjk_graph* graph)
+{
+    return guard([&] {
+        if (!graph) throw lsjk::Error(LSJK_EINVAL, "null graph");
+        set_device(*graph->ctx);
+        LSJK_CUDA(cudaGraphLaunch(graph->exec, graph->ctx->stream));
+    });
+}
+
+int lsjk_graph_destroy(lsjk_graph* graph)
+{
+    return guard([&] {
+        if (!graph) return;
+        if (graph->exec) cudaGraphExecDestroy(graph->exec);
+        if (graph->graph) cudaGraphDestroy(graph->graph);
+        delete graph;
     });
 }
 

@@ -120,11 +120,19 @@ struct KInvClass {
     DBuf<int> row_start, row_len;    // per indexed primitive (len 0: no partners)
 };
 
-// Partner entries of all K-invert rows (SoA, sorted by class, indexed prim,
-// bound desc, partner asc -- the order of kvec.cpp:17-27).
+// Partner entries of all K-invert rows (SoA). Each row (class, indexed prim)
+// holds the partners grouped by contracted shell ("segments": same K target
+// block), segments ordered by their largest bound, entries inside a segment
+// by bound desc, partner asc. The quartet set does not depend on this order
+// (every screen is a per-quartet test); the grouping lets the K kernel sum a
+// segment in registers before one atomic update.
+// Pair data are stored relative to the indexed primitive's centre R_i:
+//   P_rel = P - R_i, A_rel = R_partner - R_i
+// so FP32 arithmetic on them has no cancellation.
 struct KInvData {
     long nent = 0;
-    DBuf<double> kab, pe, px, py, pz;  // K_ab prefactor, partner exponent and centre
+    DBuf<double> kab, p, ip, px, py, pz, ax, ay, az;        // FP64 pair data; kab = K_ab / p
+    DBuf<float> kab32, p32, ip32, px32, py32, pz32, ax32, ay32, az32;  // FP32 copies
     DBuf<int> pcart;                   // partner cartIdx
     DBuf<float> pbound;                // Schwarz bound of the pair
 };
@@ -151,8 +159,18 @@ struct PairList {
     bool kinv_built = false;
 };
 
+// Launch schedules picked by the autotuner (0 = built-in default).
+struct Tune {
+    int j_chunk[kNHerm][kNHerm] = {};              // ket pairs per J CTA, per (LB, LK)
+    int k_ctas_per_sm[2][kNL][kNL][kNL][kNL] = {}; // K grid size, per pass (FP64, FP32) and class
+};
+constexpr int kTuneInts = kNHerm * kNHerm + 2 * kNL * kNL * kNL * kNL;
+
 struct Context {
     int device = 0;
+    Tune tune;
+    bool tuning = false;            // time candidate schedules on the next builds
+    DBuf<unsigned long long> tune_sink;  // counters written by timing launches
     cudaStream_t stream = nullptr;
     int precision = LSJK_PREC_MIXED;
     DBuf<double> boys64, rys64;     // quadrature tables (FP64)
@@ -169,6 +187,7 @@ struct Context {
     char* scratch_take(size_t bytes);
     void scratch_reset() { scratch_used = 0; }
     int smem_optin = 0;
+    int nsm = 148;                  // multiprocessors of the device
 };
 
 // Stream-ordered scratch: a bump allocator over a few large blocks, reset at
@@ -212,8 +231,13 @@ struct Ewald {
     std::vector<double> alpha, omega;   // terms with alpha != 0 and omega != 0
 };
 
+// densities per batched J launch
+constexpr int kJBatchMax = 4;
+
+// J for ng (1..4) densities at once; batched densities share the quartets
+// (screened with the largest |D| of the batch).
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                   const double* Dcart, double* Jcart, float thresp, float thredp);
+                   const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp);
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                     const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
                     float thresp, float thredp);

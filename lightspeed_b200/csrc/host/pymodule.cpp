@@ -194,8 +194,53 @@ PYBIND11_MODULE(_lightspeed, m)
     m.def("set_precision", [](int mode) { Engine::instance().set_precision(mode); });
     m.def("get_precision", []() { return Engine::instance().precision(); });
     m.def("stats", &stats_dict);
+    m.def("class_counts", []() {
+        // quartets per class: {"fp64"|"fp32": {"J": {(LB,LK): n}, "K": {(L1,L2,L3,L4): n}}}
+        std::vector<unsigned long long> h(2 * (25 + 81));
+        check_rc(lsjk_context_counters(Engine::instance().ctx(), h.data(), (int) h.size()), "class_counts");
+        py::dict out;
+        for (int prec = 0; prec < 2; ++prec) {
+            py::dict j, k;
+            const unsigned long long* b = h.data() + prec * (25 + 81);
+            for (int LB = 0; LB < 5; ++LB)
+                for (int LK = 0; LK < 5; ++LK)
+                    if (b[LB * 5 + LK]) j[py::make_tuple(LB, LK)] = b[LB * 5 + LK];
+            for (int c = 0; c < 81; ++c)
+                if (b[25 + c]) k[py::make_tuple(c / 27, (c / 9) % 3, (c / 3) % 3, c % 3)] = b[25 + c];
+            py::dict d;
+            d["J"] = j;
+            d["K"] = k;
+            out[prec ? "fp32" : "fp64"] = d;
+        }
+        return out;
+    });
     m.def("reset_stats", []() { check_rc(lsjk_context_reset_stats(Engine::instance().ctx()), "reset_stats"); });
     m.def("engine_version", []() { return std::string(lsjk_version()); });
+    // CUDA-graph capture of device-API builds (see include/lsjk.h)
+    struct Graph {
+        lsjk_graph* g = nullptr;
+        ~Graph() { if (g) lsjk_graph_destroy(g); }
+    };
+    py::class_<Graph, std::shared_ptr<Graph>>(m, "Graph")
+        .def("launch", [](Graph& g) { check_rc(lsjk_graph_launch(g.g), "graph launch"); },
+             py::call_guard<py::gil_scoped_release>());
+    m.def("graph_begin", []() { check_rc(lsjk_graph_begin(Engine::instance().ctx()), "graph_begin"); });
+    m.def("graph_end", []() {
+        auto g = std::make_shared<Graph>();
+        check_rc(lsjk_graph_end(Engine::instance().ctx(), &g->g), "graph_end");
+        return g;
+    });
+    m.def("set_autotune", [](bool on) { check_rc(lsjk_context_set_autotune(Engine::instance().ctx(), on ? 1 : 0),
+                                                 "set_autotune"); });
+    m.def("get_tune_table", []() {
+        std::vector<int> t(LSJK_TUNE_INTS);
+        check_rc(lsjk_context_tune_table(Engine::instance().ctx(), t.data(), (int) t.size(), 0), "tune table");
+        return t;
+    });
+    m.def("set_tune_table", [](std::vector<int> t) {
+        if (t.size() != LSJK_TUNE_INTS) throw std::runtime_error("tune table: wrong size");
+        check_rc(lsjk_context_tune_table(Engine::instance().ctx(), t.data(), (int) t.size(), 1), "tune table");
+    });
     m.def("stream_handle", []() { return (uintptr_t) lsjk_context_stream(Engine::instance().ctx()); },
           "cudaStream_t of the engine context, as an integer");
     m.def("fma_peak_tflops", [](bool fp64) {

@@ -6,7 +6,8 @@
 namespace lsjk {
 
 constexpr int kJThreads = 128;   // bra pairs per CTA (one per thread)
-constexpr int kJChunk = 512;     // ket pairs per CTA
+constexpr int kJChunk = 512;     // default ket pairs per CTA (the autotuner may pick another)
+constexpr int kJBatch = kJBatchMax;   // densities sharing one pass over the quartets
 
 struct JArgs {
     const double* bgeom;      // bra: n x 4 (p, P)
@@ -24,6 +25,9 @@ struct JArgs {
     unsigned long long* qcount32;   // FP32 quartets of this class
     int mixed;                // 1: quartets with estimate < thredp run in FP32
     float thredp;
+    int chunk;                // ket pairs per CTA (grid.y = ceil(nket / chunk))
+    int ng;                   // densities in this launch (1..kJBatch); ket records hold ng blocks
+    long jbra_stride;         // distance between the densities' bra accumulators
     int nterm;
     double alpha[4], omega[4];
     float thresp;

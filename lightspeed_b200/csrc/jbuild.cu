@@ -32,9 +32,16 @@ inline unsigned nblk(long n, int t) { return (unsigned) ((n + t - 1) / t); }
 
 // ---- 1. ket screening -------------------------------------------------------
 
+// The densities of one launch (1..kJBatch), passed by value.
+struct DSet {
+    const double* d[kJBatch];
+    int n;       // densities present
+    int slots;   // record slots (1, or kJBatch for a batched launch)
+};
+
 __global__ void k_ket_screen(const int* __restrict__ p1, const int* __restrict__ p2,
                              const float* __restrict__ bound, int n, BasisView b3, BasisView b4,
-                             int symm, const double* __restrict__ Dc, float thre,
+                             int symm, DSet D, float thre,
                              unsigned* __restrict__ key, int* __restrict__ val,
                              int* __restrict__ nkept, unsigned* __restrict__ maxbits)
 {
@@ -44,12 +51,17 @@ __global__ void k_ket_screen(const int* __restrict__ p1, const int* __restrict__
     int a1 = b3.cart[i], a2 = b4.cart[j];
     int c1 = ncart_of(b3.L[i]), c2 = ncart_of(b4.L[j]);
     int ld = b4.ncart;
+    // max |D| over the pair block (both triangles if symmetric) and, for a
+    // batched launch, over its densities: the batch screens with the union
     double v = 0.0;
-    for (int x = 0; x < c1; ++x)
-        for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a1 + x) * ld + a2 + y]));
-    if (symm)
+    for (int g = 0; g < D.n; ++g) {
+        const double* Dc = D.d[g];
         for (int x = 0; x < c1; ++x)
-            for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a2 + y) * ld + a1 + x]));
+            for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a1 + x) * ld + a2 + y]));
+        if (symm)
+            for (int x = 0; x < c1; ++x)
+                for (int y = 0; y < c2; ++y) v = fmax(v, fabs(Dc[(long) (a2 + y) * ld + a1 + x]));
+    }
     float B2 = (float) (v * (double) bound[k]);
     bool keep = B2 > thre;
     key[k] = keep ? ~__float_as_uint(B2) : 0xffffffffu;
@@ -89,11 +101,43 @@ __global__ void k_bra_count(const unsigned* __restrict__ maxbits, float thresp, 
 
 // ---- 3. ket Hermite densities -------------------------------------------------
 
+// Hermite expansion of one pair block of one density: out[t] for t < H.
+// Kept out of line so the (runtime) loop over the densities of a batch wraps
+// a call instead of the fully unrolled expansion.
 template <int L3, int L4>
-__device__ void ket_record(int i, int j, BasisView b3, BasisView b4, bool symm, const double* __restrict__ Dc,
-                           const double* __restrict__ geom, double* __restrict__ rec)
+__device__ __noinline__ void ket_herm_block(const ECoef<L3, L4>& E, const double* __restrict__ Dc, int a1, int a2,
+                                            int ld, bool symm, double scale, double pre, double* __restrict__ out)
 {
     constexpr int N3 = ncart_of(L3), N4 = ncart_of(L4), H = nherm_of(L3 + L4);
+    double Dp[N3][N4];
+#pragma unroll
+    for (int x = 0; x < N3; ++x)
+#pragma unroll
+        for (int y = 0; y < N4; ++y) {
+            double v = Dc[(long) (a1 + x) * ld + a2 + y];
+            if (symm) v += Dc[(long) (a2 + y) * ld + a1 + x];
+            Dp[x][y] = v * scale;
+        }
+#pragma unroll
+    for (int t = 0; t < H; ++t) {
+        const int tx = herm_tx(t), ty = herm_ty(t), tz = herm_tz(t);
+        double s = 0.0;
+#pragma unroll
+        for (int x = 0; x < N3; ++x)
+#pragma unroll
+            for (int y = 0; y < N4; ++y) {
+                s += E.v[0][cart_lx(L3, x)][cart_lx(L4, y)][tx] * E.v[1][cart_ly(L3, x)][cart_ly(L4, y)][ty] *
+                     E.v[2][cart_lz(L3, x)][cart_lz(L4, y)][tz] * Dp[x][y];
+            }
+        out[t] = ((tx + ty + tz) & 1 ? -pre : pre) * s;
+    }
+}
+
+template <int L3, int L4>
+__device__ void ket_record(int i, int j, BasisView b3, BasisView b4, bool symm, const DSet& DS,
+                           const double* __restrict__ geom, double* __restrict__ rec)
+{
+    constexpr int H = nherm_of(L3 + L4);
     const double q = geom[0];
     const double Q[3] = {geom[1], geom[2], geom[3]};
     const double A[3] = {b3.x[i], b3.y[i], b3.z[i]};
@@ -112,32 +156,18 @@ __device__ void ket_record(int i, int j, BasisView b3, BasisView b4, bool symm, 
     build_E<L3, L4>(q, QA, QB, E);
     const int a1 = b3.cart[i], a2 = b4.cart[j], ld = b4.ncart;
     const double scale = (symm && i == j) ? 0.5 : 1.0;
-    double Dp[N3][N4];
-#pragma unroll
-    for (int x = 0; x < N3; ++x)
-#pragma unroll
-        for (int y = 0; y < N4; ++y) {
-            double v = Dc[(long) (a1 + x) * ld + a2 + y];
-            if (symm) v += Dc[(long) (a2 + y) * ld + a1 + x];
-            Dp[x][y] = v * scale;
-        }
     const double pre = Kab / q;
     rec[0] = q;
     rec[1] = Q[0];
     rec[2] = Q[1];
     rec[3] = Q[2];
-#pragma unroll
-    for (int t = 0; t < H; ++t) {
-        const int tx = herm_tx(t), ty = herm_ty(t), tz = herm_tz(t);
-        double s = 0.0;
-#pragma unroll
-        for (int x = 0; x < N3; ++x)
-#pragma unroll
-            for (int y = 0; y < N4; ++y) {
-                s += E.v[0][cart_lx(L3, x)][cart_lx(L4, y)][tx] * E.v[1][cart_ly(L3, x)][cart_ly(L4, y)][ty] *
-                     E.v[2][cart_lz(L3, x)][cart_lz(L4, y)][tz] * Dp[x][y];
-            }
-        rec[4 + t] = ((tx + ty + tz) & 1 ? -pre : pre) * s;
+#pragma unroll 1
+    for (int g = 0; g < DS.slots; ++g) {
+        double* out = rec + 4 + g * H;
+        if (g < DS.n)
+            ket_herm_block<L3, L4>(E, DS.d[g], a1, a2, ld, symm, scale, pre, out);
+        else
+            for (int t = 0; t < H; ++t) out[t] = 0.0;   // unused slot of a partial batch
     }
 }
 
@@ -145,10 +175,10 @@ template <int LK>
 __global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__ nkept,
                            const int* __restrict__ p1, const int* __restrict__ p2,
                            const float* __restrict__ bound, const double* __restrict__ geom,
-                           BasisView b3, BasisView b4, int symm, const double* __restrict__ Dc,
+                           BasisView b3, BasisView b4, int symm, DSet Dc,
                            double* __restrict__ rec, float* __restrict__ rec32)
 {
-    constexpr int S = 4 + nherm_of(LK);
+    const int S = 4 + Dc.slots * nherm_of(LK);
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= *nkept) return;
     int src = perm[k];
@@ -169,7 +199,7 @@ __global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__
     if (rec32) {
         float* r32 = rec32 + (long) k * S;
 #pragma unroll
-        for (int t = 0; t < S; ++t) r32[t] = (float) r[t];
+        for (int t = 0; t < S; ++t) r32[t] = (float) r[t];   // S is runtime: plain loop
     }
 }
 
@@ -273,8 +303,13 @@ double j_quartet_flops(int LB, int LK)
 }
 
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                   const double* Dcart, double* Jcart, float thresp, float thredp)
+                   const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp)
 {
+    if (ng < 1 || ng > kJBatch) throw Error(LSJK_EINVAL, "coulomb_build: 1..4 densities per launch");
+    DSet DS{};
+    for (int g = 0; g < ng; ++g) DS.d[g] = Dcart[g];
+    DS.n = ng;
+    DS.slots = ng == 1 ? 1 : kJBatch;
     cudaStream_t s = ctx->stream;
     const Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
     // thresp / max12 (truncate_ket threshold), float as in the reference call
@@ -302,22 +337,22 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
         int* val = take<int>(ctx, n);
         int* perm = take<int>(ctx, n);
         k_ket_screen<<<nblk(n, 256), 256, 0, s>>>(jk.p1.p, jk.p2.p, jk.bound.p, n, b3->view(), b4->view(),
-                                                 pl34->symm ? 1 : 0, Dcart, thre_ket, key, val, nket + LK,
+                                                 pl34->symm ? 1 : 0, DS, thre_ket, key, val, nket + LK,
                                                  maxbits + LK);
         size_t tmp = 0;
         LSJK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, keys, val, perm, n, 0, 32, s));
         void* t = ctx->scratch_take(tmp);
         LSJK_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, key, keys, val, perm, n, 0, 32, s));
-        krec[LK] = take<double>(ctx, (long) n * (4 + nherm_of(LK)));
-        if (mixed) krec32[LK] = take<float>(ctx, (long) n * (4 + nherm_of(LK)));
+        krec[LK] = take<double>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
+        if (mixed) krec32[LK] = take<float>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
         kbound[LK] = take<float>(ctx, n);
         k_ket_bounds<<<nblk(n, 256), 256, 0, s>>>(keys, nket + LK, kbound[LK]);
         switch (LK) {
-        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
-        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
-        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
-        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
-        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, Dcart, krec[LK], krec32[LK]); break;
+        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
+        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
+        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
+        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
+        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
         }
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches += 7;
@@ -340,8 +375,8 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
     for (int LB = 0; LB < kNHerm; ++LB) {
         int n = pl12->jb[LB].n;
         if (!n) continue;
-        jbra[LB] = take<double>(ctx, (long) n * nherm_of(LB));
-        LSJK_CUDA(cudaMemsetAsync(jbra[LB], 0, sizeof(double) * n * nherm_of(LB), s));
+        jbra[LB] = take<double>(ctx, (long) DS.slots * n * nherm_of(LB));
+        LSJK_CUDA(cudaMemsetAsync(jbra[LB], 0, sizeof(double) * DS.slots * n * nherm_of(LB), s));
     }
     for (int LB = 0; LB < kNHerm; ++LB) {
         const JBraClass& jb = pl12->jb[LB];
@@ -365,37 +400,72 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             A.boys32 = ctx->boys32.p + (long) (LB + LK) * LSJK_BOYS_NBIN * 8;
             A.mixed = mixed ? 1 : 0;
             A.thredp = thredp;
+            A.chunk = ctx->tune.j_chunk[LB][LK] > 0 ? ctx->tune.j_chunk[LB][LK] : kJChunk;
+            A.ng = ng;
+            A.jbra_stride = (long) jb.n * nherm_of(LB);
             A.nterm = (int) ew.alpha.size();
             for (int t = 0; t < A.nterm; ++t) {
                 A.alpha[t] = ew.alpha[t];
                 A.omega[t] = ew.omega[t];
             }
             A.thresp = thresp;
-            switch (LB) {
-            case 0: launch_j_row<0>(ctx, A, LK, jb.n, jk.n); break;
-            case 1: launch_j_row<1>(ctx, A, LK, jb.n, jk.n); break;
-            case 2: launch_j_row<2>(ctx, A, LK, jb.n, jk.n); break;
-            case 3: launch_j_row<3>(ctx, A, LK, jb.n, jk.n); break;
-            case 4: launch_j_row<4>(ctx, A, LK, jb.n, jk.n); break;
+            auto launch = [&](const JArgs& X) {
+                switch (LB) {
+                case 0: launch_j_row<0>(ctx, X, LK, jb.n, jk.n); break;
+                case 1: launch_j_row<1>(ctx, X, LK, jb.n, jk.n); break;
+                case 2: launch_j_row<2>(ctx, X, LK, jb.n, jk.n); break;
+                case 3: launch_j_row<3>(ctx, X, LK, jb.n, jk.n); break;
+                case 4: launch_j_row<4>(ctx, X, LK, jb.n, jk.n); break;
+                }
+            };
+            if (ctx->tuning) {
+                // autotuner: time the candidate ket chunk sizes on scratch outputs
+                static const int cand[] = {128, 256, 512, 1024, 2048, 4096};
+                JArgs T = A;
+                T.jbra = take<double>(ctx, (long) DS.slots * jb.n * nherm_of(LB));
+                T.qcount = T.qcount32 = ctx->tune_sink.p;
+                float best = 1e30f;
+                for (int c : cand) {
+                    T.chunk = c;
+                    float ms = 1e30f;
+                    for (int rep = 0; rep < 2; ++rep) {
+                        LSJK_CUDA(cudaEventRecord(ctx->ev0, s));
+                        launch(T);
+                        LSJK_CUDA(cudaEventRecord(ctx->ev1, s));
+                        LSJK_CUDA(cudaEventSynchronize(ctx->ev1));
+                        float t = 0.f;
+                        LSJK_CUDA(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+                        ms = std::min(ms, t);
+                    }
+                    if (ms < best) {
+                        best = ms;
+                        ctx->tune.j_chunk[LB][LK] = c;
+                    }
+                }
+                A.chunk = ctx->tune.j_chunk[LB][LK];
             }
+            launch(A);
         }
     }
 
-    // 5. back to Cartesian
-    for (int LB = 0; LB < kNHerm; ++LB) {
-        const JBraClass& jb = pl12->jb[LB];
-        if (!jb.n) continue;
-        unsigned g = nblk(jb.n, 128);
-        switch (LB) {
-        case 0: k_herm_to_cart<0><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
-        case 1: k_herm_to_cart<1><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
-        case 2: k_herm_to_cart<2><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
-        case 3: k_herm_to_cart<3><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
-        case 4: k_herm_to_cart<4><<<g, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jbra[LB], Jcart); break;
+    // 5. back to Cartesian, per density
+    for (int g = 0; g < ng; ++g)
+        for (int LB = 0; LB < kNHerm; ++LB) {
+            const JBraClass& jb = pl12->jb[LB];
+            if (!jb.n) continue;
+            unsigned gr = nblk(jb.n, 128);
+            const double* jt = jbra[LB] + (long) g * jb.n * nherm_of(LB);
+            double* Jc = Jcart[g];
+            switch (LB) {
+            case 0: k_herm_to_cart<0><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 1: k_herm_to_cart<1><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 2: k_herm_to_cart<2><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 3: k_herm_to_cart<3><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 4: k_herm_to_cart<4><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            }
+            LSJK_CUDA(cudaGetLastError());
+            ctx->stats.kernel_launches++;
         }
-        LSJK_CUDA(cudaGetLastError());
-        ctx->stats.kernel_launches++;
-    }
 }
 
 } // namespace lsjk

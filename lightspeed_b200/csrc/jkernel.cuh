@@ -11,12 +11,13 @@ namespace lsjk {
 
 
 
-// One J quartet (bra pair in registers, ket record r) accumulated into jp.
-template <int LB, int LK>
+// One J quartet (bra pair in registers, ket record r) accumulated into jp,
+// for the NG densities of the record (the Hermite integrals R_tuv are shared).
+template <int LB, int LK, int NG>
 __device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, double p, double Px, double Py,
-                                            double Pz, const double* __restrict__ r, double* jp)
+                                            double Pz, const double* __restrict__ r, double (*jp)[nherm_of(LB)])
 {
-    constexpr int L = LB + LK;
+    constexpr int L = LB + LK, HK = nherm_of(LK);
     const double q = r[0];
     const double X = Px - r[1], Y = Py - r[2], Z = Pz - r[3];
     const double R2 = X * X + Y * Y + Z * Z;
@@ -41,26 +42,30 @@ __device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, d
             a[n] = pw * F[n];
             pw *= m2r;
         }
-        jq_dispatch<LB, LK>(a, X, Y, Z, r + 4, jp);
+#pragma unroll
+        for (int g = 0; g < NG; ++g)
+            if (g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r + 4 + g * HK, jp[g]);
     }
 }
 
 // The same quartet in FP32 (geometry differences formed in FP64, everything
 // else in FP32), added to the FP64 accumulators.
-template <int LB, int LK>
+template <int LB, int LK, int NG>
 __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, float p, double Px, double Py,
                                             double Pz, const double* __restrict__ r, const float* __restrict__ r32,
-                                            double* jp)
+                                            double (*jp)[nherm_of(LB)])
 {
-    constexpr int L = LB + LK, HB = nherm_of(LB);
+    constexpr int L = LB + LK, HB = nherm_of(LB), HK = nherm_of(LK);
     const float q = r32[0];
     const float X = (float) (Px - r[1]), Y = (float) (Py - r[2]), Z = (float) (Pz - r[3]);
     const float R2 = X * X + Y * Y + Z * Z;
     const float rs = rsqrtf(p + q);
     const float rho = p * q * (rs * rs);
-    float jq[HB];
+    float jq[NG][HB];
 #pragma unroll
-    for (int t = 0; t < HB; ++t) jq[t] = 0.0f;
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+        for (int t = 0; t < HB; ++t) jq[g][t] = 0.0f;
     for (int tm = 0; tm < A.nterm; ++tm) {
         const float om = (float) A.omega[tm];
         float d2 = 1.0f, f = (float) A.alpha[tm] * rs;
@@ -80,22 +85,26 @@ __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, fl
             a[n] = pw * F[n];
             pw *= m2r;
         }
-        jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4, jq);
+#pragma unroll
+        for (int g = 0; g < NG; ++g)
+            if (g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4 + g * HK, jq[g]);
     }
 #pragma unroll
-    for (int t = 0; t < HB; ++t) jp[t] += (double) jq[t];
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+        for (int t = 0; t < HB; ++t) jp[g][t] += (double) jq[g][t];
 }
 
-template <int LB, int LK>
+template <int LB, int LK, int NG>
 __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 {
-    constexpr int HB = nherm_of(LB), S = 4 + nherm_of(LK);
+    constexpr int HB = nherm_of(LB), S = 4 + NG * nherm_of(LK);
     __shared__ __align__(128) double tab[LSJK_BOYS_NBIN * 8];
     __shared__ __align__(128) float tab32[LSJK_BOYS_NBIN * 8];
     __shared__ __align__(8) uint64_t mbar[2];
     const int nb = *A.nbra, nk = *A.nket;
     const int i0 = blockIdx.x * kJThreads;
-    const int j0 = blockIdx.y * kJChunk;
+    const int j0 = blockIdx.y * A.chunk;
     if (i0 >= nb || j0 >= nk) return;
     const float B0 = A.bbound[i0];
     if (B0 * A.kbound[j0] < A.thresp) return;
@@ -115,11 +124,13 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
     }
     const float p32 = (float) p;
     const float thr_dp = A.mixed ? A.thredp : 0.0f;
-    double jp[HB];
+    double jp[NG][HB];
 #pragma unroll
-    for (int t = 0; t < HB; ++t) jp[t] = 0.0;
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+        for (int t = 0; t < HB; ++t) jp[g][t] = 0.0;
     long nq = 0, nq32 = 0;
-    const int j1 = min(j0 + kJChunk, nk);
+    const int j1 = min(j0 + A.chunk, nk);
     for (int j = j0; j < j1; ++j) {
         const float Bj = A.kbound[j];
         if (B0 * Bj < A.thresp) break;
@@ -131,20 +142,22 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         if (__any_sync(0xffffffffu, dp)) {
             if (dp) {
                 ++nq;
-                j_quartet64<LB, LK>(A, tab, p, Px, Py, Pz, r, jp);
+                j_quartet64<LB, LK, NG>(A, tab, p, Px, Py, Pz, r, jp);
             }
         }
         if (__any_sync(0xffffffffu, sp)) {
             if (sp) {
                 ++nq32;
-                j_quartet32<LB, LK>(A, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
+                j_quartet32<LB, LK, NG>(A, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
             }
         }
     }
     if (act) {
 #pragma unroll
-        for (int t = 0; t < HB; ++t)
-            if (jp[t] != 0.0) atomicAdd(&A.jbra[(long) i * HB + t], jp[t]);
+        for (int g = 0; g < NG; ++g)
+#pragma unroll
+            for (int t = 0; t < HB; ++t)
+                if (jp[g][t] != 0.0) atomicAdd(&A.jbra[g * A.jbra_stride + (long) i * HB + t], jp[g][t]);
     }
     // quartet counts for the statistics
     for (int o = 16; o > 0; o >>= 1) {
@@ -161,8 +174,11 @@ template <int LB, int LK>
 void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full)
 {
     if (nbra_full == 0 || nket_full == 0) return;
-    dim3 grid((nbra_full + kJThreads - 1) / kJThreads, (nket_full + kJChunk - 1) / kJChunk);
-    k_coulomb<LB, LK><<<grid, kJThreads, 0, ctx->stream>>>(A);
+    dim3 grid((nbra_full + kJThreads - 1) / kJThreads, (nket_full + A.chunk - 1) / A.chunk);
+    if (A.ng <= 1)
+        k_coulomb<LB, LK, 1><<<grid, kJThreads, 0, ctx->stream>>>(A);
+    else
+        k_coulomb<LB, LK, kJBatch><<<grid, kJThreads, 0, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
 }

@@ -8,6 +8,8 @@ namespace lsjk {
 constexpr int kKThreads = 128;
 constexpr int kKWarps = kKThreads / 32;
 
+// One (prim2, prim4) task: the K-invert rows of prim2 (partners 1) and prim4
+// (partners 3) and the largest |D24| over the pair's Cartesian block.
 struct KTask {
     int i2, i4;
     double dmax;
@@ -20,46 +22,48 @@ struct KScalars {
     float thre12, thre34;
 };
 
+// K-invert partner data of one pair list, in one precision.
+template <typename R>
+struct KRows {
+    const R *kab, *p, *ip, *px, *py, *pz, *ax, *ay, *az;
+};
+
 struct KArgs {
     const KTask* tasks;
     const int* ntask;
     unsigned* queue;
-    const int* r12s;
+    const int* r12s;          // rows of prim2 in class (L2 indexed, L1 partner)
     const int* r12l;
-    const int* r34s;
+    const int* r34s;          // rows of prim4 in class (L4, L3)
     const int* r34l;
-    const double *kab12, *e12, *x12, *y12, *z12;
+    KRows<double> d12, d34;
+    KRows<float> f12, f34;
     const int* cart12;
     const float* b12;
-    const double *kab34, *e34, *x34, *y34, *z34;
     const int* cart34;
     const float* b34;
-    BasisView b2, b4;
+    BasisView b2, b4;         // indexed primitives (centres, cartIdx)
     const double* Dc;
     int ld4;
     double* Kc;
     int ld3;
     int flip;
-    float thresp;
+    // this pass computes quartets with thr_lo <= estimate < thr_hi
+    float thr_lo, thr_hi;
     const KScalars* sc;
-    const double* rys;     // table block of this rule
-    const double* asym_t;
-    const double* asym_w;
+    const void* rys;          // table block of this rule, in the pass precision
+    const void* asym_t;
+    const void* asym_w;
     int nbin;
     double tmax;
     int* status;
-    unsigned long long* qcount;     // FP64 quartets of this class
-    unsigned long long* qcount32;   // FP32 quartets of this class
-    const float* rys32;             // FP32 copy of the table block
-    const float* asym_t32;
-    const float* asym_w32;
-    int mixed;                      // 1: estimate < thredp runs in FP32
-    float thredp;
+    unsigned long long* qcount;
     int nterm;
     double alpha[4], omega[4];
 };
 
+// Launch the FP64 (fp32 = false) or FP32 (fp32 = true) pass of one class.
 template <int L1, int L2, int L3, int L4>
-void launch_k(Context* ctx, const KArgs& A, long cap);
+void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32);
 
 } // namespace lsjk

@@ -53,14 +53,14 @@ __global__ void k_kscalars(KScalars* S, float thresp, double maxb12, double maxb
     S->thre34 = (float) ((double) thresp / (maxb12 * d));
 }
 
-struct KRows {
+struct KRowTables {
     const int* start[kNL][kNL];   // [L_indexed][L_partner]
     const int* len[kNL][kNL];
 };
 
 struct TaskGenArgs {
     BasisView b2, b4;
-    KRows r12, r34;
+    KRowTables r12, r34;
     const float* pb12;
     const float* pb34;
     const double* Dc;
@@ -112,38 +112,38 @@ __global__ void k_task_gen(TaskGenArgs A)
 
 // Runtime (L1,L2,L3,L4) -> template dispatch.
 template <int L1, int L2, int L3>
-void launch_k4(Context* ctx, const KArgs& A, long cap, int L4)
+void launch_k4(Context* ctx, const KArgs& A, long cap, int L4, bool fp32)
 {
     switch (L4) {
-    case 0: launch_k<L1, L2, L3, 0>(ctx, A, cap); break;
-    case 1: launch_k<L1, L2, L3, 1>(ctx, A, cap); break;
-    case 2: launch_k<L1, L2, L3, 2>(ctx, A, cap); break;
+    case 0: launch_k<L1, L2, L3, 0>(ctx, A, cap, fp32); break;
+    case 1: launch_k<L1, L2, L3, 1>(ctx, A, cap, fp32); break;
+    case 2: launch_k<L1, L2, L3, 2>(ctx, A, cap, fp32); break;
     }
 }
 template <int L1, int L2>
-void launch_k3(Context* ctx, const KArgs& A, long cap, int L3, int L4)
+void launch_k3(Context* ctx, const KArgs& A, long cap, int L3, int L4, bool fp32)
 {
     switch (L3) {
-    case 0: launch_k4<L1, L2, 0>(ctx, A, cap, L4); break;
-    case 1: launch_k4<L1, L2, 1>(ctx, A, cap, L4); break;
-    case 2: launch_k4<L1, L2, 2>(ctx, A, cap, L4); break;
+    case 0: launch_k4<L1, L2, 0>(ctx, A, cap, L4, fp32); break;
+    case 1: launch_k4<L1, L2, 1>(ctx, A, cap, L4, fp32); break;
+    case 2: launch_k4<L1, L2, 2>(ctx, A, cap, L4, fp32); break;
     }
 }
 template <int L1>
-void launch_k2(Context* ctx, const KArgs& A, long cap, int L2, int L3, int L4)
+void launch_k2(Context* ctx, const KArgs& A, long cap, int L2, int L3, int L4, bool fp32)
 {
     switch (L2) {
-    case 0: launch_k3<L1, 0>(ctx, A, cap, L3, L4); break;
-    case 1: launch_k3<L1, 1>(ctx, A, cap, L3, L4); break;
-    case 2: launch_k3<L1, 2>(ctx, A, cap, L3, L4); break;
+    case 0: launch_k3<L1, 0>(ctx, A, cap, L3, L4, fp32); break;
+    case 1: launch_k3<L1, 1>(ctx, A, cap, L3, L4, fp32); break;
+    case 2: launch_k3<L1, 2>(ctx, A, cap, L3, L4, fp32); break;
     }
 }
-void launch_k1(Context* ctx, const KArgs& A, long cap, int L1, int L2, int L3, int L4)
+void launch_k1(Context* ctx, const KArgs& A, long cap, int L1, int L2, int L3, int L4, bool fp32)
 {
     switch (L1) {
-    case 0: launch_k2<0>(ctx, A, cap, L2, L3, L4); break;
-    case 1: launch_k2<1>(ctx, A, cap, L2, L3, L4); break;
-    case 2: launch_k2<2>(ctx, A, cap, L2, L3, L4); break;
+    case 0: launch_k2<0>(ctx, A, cap, L2, L3, L4, fp32); break;
+    case 1: launch_k2<1>(ctx, A, cap, L2, L3, L4, fp32); break;
+    case 2: launch_k2<2>(ctx, A, cap, L2, L3, L4, fp32); break;
     }
 }
 
@@ -166,6 +166,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     float thresp, float thredp)
 {
     cudaStream_t s = ctx->stream;
+    const int b1c = pl12->b1->ncart;
     const Basis *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
     // global max |D24| (exchange.cpp:48-52) and the K-invert thresholds
     KScalars* sc = take<KScalars>(ctx, 1);
@@ -191,12 +192,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
     int* ntask = take<int>(ctx, kNCombo);
-    unsigned* queue = take<unsigned>(ctx, kNCombo);
+    unsigned* queue = take<unsigned>(ctx, 2 * kNCombo);
     unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
     unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
     const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
     LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
-    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * kNCombo, s));
+    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo, s));
 
     TaskGenArgs G{};
     G.b2 = b2->view();
@@ -239,17 +240,24 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     KArgs A{};
                     A.tasks = tasks + off[c];
                     A.ntask = ntask + c;
-                    A.queue = queue + c;
                     A.r12s = pl12->kinv[L2][L1].row_start.p;
                     A.r12l = pl12->kinv[L2][L1].row_len.p;
                     A.r34s = pl34->kinv[L4][L3].row_start.p;
                     A.r34l = pl34->kinv[L4][L3].row_len.p;
                     const KInvData& d12 = pl12->kdat;
                     const KInvData& d34 = pl34->kdat;
-                    A.kab12 = d12.kab.p; A.e12 = d12.pe.p; A.x12 = d12.px.p; A.y12 = d12.py.p; A.z12 = d12.pz.p;
-                    A.cart12 = d12.pcart.p; A.b12 = d12.pbound.p;
-                    A.kab34 = d34.kab.p; A.e34 = d34.pe.p; A.x34 = d34.px.p; A.y34 = d34.py.p; A.z34 = d34.pz.p;
-                    A.cart34 = d34.pcart.p; A.b34 = d34.pbound.p;
+                    A.d12 = KRows<double>{d12.kab.p, d12.p.p, d12.ip.p, d12.px.p, d12.py.p, d12.pz.p,
+                                          d12.ax.p, d12.ay.p, d12.az.p};
+                    A.d34 = KRows<double>{d34.kab.p, d34.p.p, d34.ip.p, d34.px.p, d34.py.p, d34.pz.p,
+                                          d34.ax.p, d34.ay.p, d34.az.p};
+                    A.f12 = KRows<float>{d12.kab32.p, d12.p32.p, d12.ip32.p, d12.px32.p, d12.py32.p,
+                                         d12.pz32.p, d12.ax32.p, d12.ay32.p, d12.az32.p};
+                    A.f34 = KRows<float>{d34.kab32.p, d34.p32.p, d34.ip32.p, d34.px32.p, d34.py32.p,
+                                         d34.pz32.p, d34.ax32.p, d34.ay32.p, d34.az32.p};
+                    A.cart12 = d12.pcart.p;
+                    A.b12 = d12.pbound.p;
+                    A.cart34 = d34.pcart.p;
+                    A.b34 = d34.pbound.p;
                     A.b2 = b2->view();
                     A.b4 = b4->view();
                     A.Dc = Dcart;
@@ -257,27 +265,68 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.Kc = Kcart;
                     A.ld3 = b3->ncart;
                     A.flip = flip_ok ? 1 : 0;
-                    A.thresp = thresp;
                     A.sc = sc;
-                    A.rys = ctx->rys64.p + kRysOffset[NR];
-                    A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
-                    A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
                     A.nbin = kRysNbin[NR];
                     A.tmax = kRysTmax[NR];
                     A.status = ctx->status.p;
-                    A.qcount = qcnt + c;
-                    A.qcount32 = qcnt32 + c;
-                    A.rys32 = ctx->rys32.p + kRysOffset[NR];
-                    A.asym_t32 = ctx->rys_asym32.p + NR * LSJK_RYS_NMAX;
-                    A.asym_w32 = ctx->rys_asym32.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
-                    A.mixed = mixed ? 1 : 0;
-                    A.thredp = thredp;
                     A.nterm = (int) ew.alpha.size();
                     for (int t = 0; t < A.nterm; ++t) {
                         A.alpha[t] = ew.alpha[t];
                         A.omega[t] = ew.omega[t];
                     }
-                    launch_k1(ctx, A, cap, L1, L2, L3, L4);
+                    const float inf = __builtin_huge_valf();
+                    // FP64 pass: estimate >= thredp (mixed) or >= thresp (FP64 mode)
+                    A.queue = queue + c;
+                    A.thr_lo = mixed ? thredp : thresp;
+                    A.thr_hi = inf;
+                    A.rys = ctx->rys64.p + kRysOffset[NR];
+                    A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
+                    A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                    A.qcount = qcnt + c;
+                    auto tune = [&](const KArgs& X, bool fp32) {
+                        // autotuner: time candidate grid sizes on scratch outputs
+                        static const int cand[] = {2, 4, 8, 16, 32};
+                        KArgs T = X;
+                        T.Kc = take<double>(ctx, (size_t) b1c * b3->ncart);
+                        T.qcount = ctx->tune_sink.p;
+                        int& slot = ctx->tune.k_ctas_per_sm[fp32 ? 1 : 0][L1][L2][L3][L4];
+                        float best = 1e30f;
+                        int bestc = 16;
+                        for (int cnd : cand) {
+                            slot = cnd;
+                            float ms = 1e30f;
+                            for (int rep = 0; rep < 2; ++rep) {
+                                LSJK_CUDA(cudaMemsetAsync(T.queue, 0, sizeof(unsigned), s));
+                                LSJK_CUDA(cudaEventRecord(ctx->ev0, s));
+                                launch_k1(ctx, T, cap, L1, L2, L3, L4, fp32);
+                                LSJK_CUDA(cudaEventRecord(ctx->ev1, s));
+                                LSJK_CUDA(cudaEventSynchronize(ctx->ev1));
+                                float t = 0.f;
+                                LSJK_CUDA(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+                                ms = std::min(ms, t);
+                            }
+                            if (ms < best) {
+                                best = ms;
+                                bestc = cnd;
+                            }
+                        }
+                        slot = bestc;
+                        LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned), s));
+                    };
+                    if (ctx->tuning) tune(A, false);
+                    launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
+                    if (mixed) {
+                        // FP32 pass: thresp <= estimate < thredp
+                        A.queue = queue + kNCombo + c;
+                        A.thr_lo = thresp;
+                        A.thr_hi = thredp;
+                        A.rys = ctx->rys32.p + kRysOffset[NR];
+                        A.asym_t = ctx->rys_asym32.p + NR * LSJK_RYS_NMAX;
+                        A.asym_w = ctx->rys_asym32.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                        A.qcount = qcnt32 + c;
+                        if (ctx->tuning) tune(A, true);
+                        launch_k1(ctx, A, cap, L1, L2, L3, L4, true);
+                    }
                 }
 }
 

@@ -11,13 +11,13 @@
 #include "kkernel.cuh"
 
 namespace lsjk {
-template void launch_k<LSJK_L1, LSJK_L2, 0, 0>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 0, 1>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 0, 2>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 1, 0>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 1, 1>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 1, 2>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 2, 0>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 2, 1>(Context*, const KArgs&, long);
-template void launch_k<LSJK_L1, LSJK_L2, 2, 2>(Context*, const KArgs&, long);
+template void launch_k<LSJK_L1, LSJK_L2, 0, 0>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 0, 1>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 0, 2>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 1, 0>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 1, 1>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 1, 2>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 2, 0>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 2, 1>(Context*, const KArgs&, long, bool);
+template void launch_k<LSJK_L1, LSJK_L2, 2, 2>(Context*, const KArgs&, long, bool);
 } // namespace lsjk

@@ -1,8 +1,23 @@
-// The K kernel: one template per class (L1 L2|L3 L4). Included only by
-// kinst.cu, which is compiled once per (L1, L2) with the matching generated
-// quartet header so the 81 classes build in parallel.
+// The K kernel: one template per class (L1 L2|L3 L4) and precision. Included
+// only by kinst.cu, which is compiled once per (L1, L2) with the matching
+// generated quartet header so the classes build in parallel.
+//
+// Work unit: one (prim2, prim4) task, taken by a warp from a device queue.
+// The 32 lanes own 32 consecutive partners 3 of prim4 (their pair data stay
+// in registers for the whole task); the warp walks the partners 1 of prim2,
+// which are staged 32 at a time into a per-warp shared-memory ring by
+// cp.async (the next 32 are in flight while the current 32 are used) and read
+// as broadcasts. Partners 1 come grouped by contracted shell, so a lane sums
+// the quartets of one shell segment -- same K13 target block -- in registers
+// and issues one FP64 atomic per element when the segment ends.
+// Screens (per quartet, exactly the reference's set):
+//   bound12 >= thre12, bound34 >= thre34,
+//   thr_lo <= double(float(bound12*bound34)) * max|D24 block| < thr_hi
+// where [thr_lo, thr_hi) is [thresp, inf) in FP64 mode and splits at thredp
+// into an FP64 pass and an FP32 pass in mixed mode.
 #pragma once
 #include <algorithm>
+#include <type_traits>
 #include "kargs.cuh"
 #include "lsjk_device.cuh"
 
@@ -10,102 +25,86 @@ namespace lsjk {
 
 constexpr double kTwoPi52K = 34.986836655249725693;   // 2 pi^(5/2)
 
-// Geometry of one K quartet, shared by both precisions (FP64).
-struct KGeom {
-    double p, q, ip, iq, Px, Py, Pz, Qx, Qy, Qz, Ax, Ay, Az, Bx, By, Bz, Cx, Cy, Cz, Dx, Dy, Dz, kab;
+// Smallest float x with double(x) * dmax >= thr. For non-negative float
+// products b = float(bound12 * bound34) the reference's screen
+// double(b) * dmax >= thr is then exactly b >= x (the map x -> double(x)*dmax
+// is monotone), so each quartet is screened with one float compare.
+__device__ __forceinline__ float float_threshold(double thr, double dmax)
+{
+    if (!(thr > 0.0)) return 0.0f;
+    if (!(dmax > 0.0)) return __int_as_float(0x7f800000);   // +inf: nothing passes
+    float x = (float) (thr / dmax);
+    for (int it = 0; it < 8 && (double) x * dmax < thr; ++it) x = nextafterf(x, __int_as_float(0x7f800000));
+    for (int it = 0; it < 8 && x > 0.0f && (double) nextafterf(x, 0.0f) * dmax >= thr; ++it) x = nextafterf(x, 0.0f);
+    return x;
+}
+
+// One partner-1 entry as staged in shared memory (80 / 48 bytes).
+template <typename R>
+struct alignas(16) KEnt {
+    R kab, p, ip, px, py, pz, ax, ay, az;
+    float b;
+    int c;
 };
 
-template <int L1, int L2, int L3, int L4>
-__device__ __forceinline__ void k_quartet64(const KArgs& A, const double* tab, const KGeom& g,
-                                            const double* Dblk, double* KV)
+// Lane l copies entry kb + l of the row (if it exists) into dst[l].
+template <typename R>
+__device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const float* __restrict__ b,
+                                          const int* __restrict__ cart, int s12, int kb, int n12, int lane)
 {
-    constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
-    const double p = g.p, q = g.q, ip = g.ip, iq = g.iq;
-    const double ipq = 1.0 / (p + q);
-    const double rho = p * q * ipq;
-    const double PQx = g.Px - g.Qx, PQy = g.Py - g.Qy, PQz = g.Pz - g.Qz;
-    const double R2 = PQx * PQx + PQy * PQy + PQz * PQz;
-    const double pref = kTwoPi52K * g.kab * ip * iq * sqrt(ipq);
-    for (int tm = 0; tm < A.nterm; ++tm) {
-        const double om = A.omega[tm];
-        double d2 = 1.0, f = A.alpha[tm] * pref;
-        if (om != -1.0) {
-            const double w2 = om * om;
-            d2 = w2 / (rho + w2);
-            f *= sqrt(d2);
-        }
-        double t2[NR], w[NR];
-        rys_eval<NR, double>(rho * d2 * R2, tab, A.nbin, A.tmax, A.asym_t, A.asym_w, t2, w);
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            const double u = t2[r] * d2 * ipq;
-            const double qu = q * u, pu = p * u;
-            kq_dispatch<L1, L2, L3, L4>(
-                (g.Px - g.Ax) - qu * PQx, (g.Py - g.Ay) - qu * PQy, (g.Pz - g.Az) - qu * PQz,
-                (g.Qx - g.Cx) + pu * PQx, (g.Qy - g.Cy) + pu * PQy, (g.Qz - g.Cz) + pu * PQz,
-                0.5 * u, 0.5 * ip * (1.0 - qu), 0.5 * iq * (1.0 - pu),
-                g.Ax - g.Bx, g.Ay - g.By, g.Az - g.Bz, g.Cx - g.Dx, g.Cy - g.Dy, g.Cz - g.Dz,
-                f * w[r], Dblk, KV);
-        }
+    if (kb + lane >= n12) return;
+    const int e = s12 + kb + lane;
+    KEnt<R>* o = dst + lane;
+    if constexpr (sizeof(R) == 8) {
+        cp_async8(&o->kab, d.kab + e);
+        cp_async8(&o->p, d.p + e);
+        cp_async8(&o->ip, d.ip + e);
+        cp_async8(&o->px, d.px + e);
+        cp_async8(&o->py, d.py + e);
+        cp_async8(&o->pz, d.pz + e);
+        cp_async8(&o->ax, d.ax + e);
+        cp_async8(&o->ay, d.ay + e);
+        cp_async8(&o->az, d.az + e);
+    } else {
+        cp_async4(&o->kab, d.kab + e);
+        cp_async4(&o->p, d.p + e);
+        cp_async4(&o->ip, d.ip + e);
+        cp_async4(&o->px, d.px + e);
+        cp_async4(&o->py, d.py + e);
+        cp_async4(&o->pz, d.pz + e);
+        cp_async4(&o->ax, d.ax + e);
+        cp_async4(&o->ay, d.ay + e);
+        cp_async4(&o->az, d.az + e);
     }
+    cp_async4(&o->b, b + e);
+    cp_async4(&o->c, cart + e);
 }
 
-// FP32 quartet: geometry differences formed in FP64, the rest in FP32.
-template <int L1, int L2, int L3, int L4>
-__device__ __forceinline__ void k_quartet32(const KArgs& A, const float* tab, const KGeom& g,
-                                            const float* Dblk, float* KV)
-{
-    constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
-    const float p = (float) g.p, q = (float) g.q, ip = (float) g.ip, iq = (float) g.iq;
-    const float ipq = 1.0f / (p + q);
-    const float rho = p * q * ipq;
-    const float PQx = (float) (g.Px - g.Qx), PQy = (float) (g.Py - g.Qy), PQz = (float) (g.Pz - g.Qz);
-    const float PAx = (float) (g.Px - g.Ax), PAy = (float) (g.Py - g.Ay), PAz = (float) (g.Pz - g.Az);
-    const float QCx = (float) (g.Qx - g.Cx), QCy = (float) (g.Qy - g.Cy), QCz = (float) (g.Qz - g.Cz);
-    const float ABx = (float) (g.Ax - g.Bx), ABy = (float) (g.Ay - g.By), ABz = (float) (g.Az - g.Bz);
-    const float CDx = (float) (g.Cx - g.Dx), CDy = (float) (g.Cy - g.Dy), CDz = (float) (g.Cz - g.Dz);
-    const float R2 = PQx * PQx + PQy * PQy + PQz * PQz;
-    const float pref = (float) (kTwoPi52K * g.kab) * ip * iq * sqrtf(ipq);
-    for (int tm = 0; tm < A.nterm; ++tm) {
-        const float om = (float) A.omega[tm];
-        float d2 = 1.0f, f = (float) A.alpha[tm] * pref;
-        if (A.omega[tm] != -1.0) {
-            const float w2 = om * om;
-            d2 = w2 / (rho + w2);
-            f *= sqrtf(d2);
-        }
-        float t2[NR], w[NR];
-        rys_eval<NR, float>(rho * d2 * R2, tab, A.nbin, (float) A.tmax, A.asym_t32, A.asym_w32, t2, w);
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            const float u = t2[r] * d2 * ipq;
-            const float qu = q * u, pu = p * u;
-            kq_dispatch<L1, L2, L3, L4>(PAx - qu * PQx, PAy - qu * PQy, PAz - qu * PQz,
-                                        QCx + pu * PQx, QCy + pu * PQy, QCz + pu * PQz,
-                                        0.5f * u, 0.5f * ip * (1.0f - qu), 0.5f * iq * (1.0f - pu),
-                                        ABx, ABy, ABz, CDx, CDy, CDz, f * w[r], Dblk, KV);
-        }
-    }
-}
-
-template <int L1, int L2, int L3, int L4>
+template <int L1, int L2, int L3, int L4, typename R>
 __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
-    extern __shared__ __align__(128) double tab[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    constexpr bool FP64 = std::is_same<R, double>::value;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R* tab = reinterpret_cast<R*>(smem_raw);
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ KEnt<R> ring_all[kKWarps][2][32];
     const int ntask = *A.ntask;
     if (ntask == 0) return;
-    const unsigned nco = (unsigned) (2 * NR * A.nbin * 8);
-    float* tab32 = reinterpret_cast<float*>(tab + nco);
-    if (!stage_bulk(tab, A.rys, nco * (unsigned) sizeof(double), &mbar[0], A.status)) return;
-    if (A.mixed && !stage_bulk(tab32, A.rys32, nco * (unsigned) sizeof(float), &mbar[1], A.status)) return;
+    const unsigned bytes = (unsigned) (2 * NR * A.nbin * 8 * sizeof(R));
+    if (!stage_bulk(tab, A.rys, bytes, &mbar, A.status)) return;
+    const R* asym_t = static_cast<const R*>(A.asym_t);
+    const R* asym_w = static_cast<const R*>(A.asym_w);
+    const R tmax = (R) A.tmax;
 
+    const KRows<R> d12 = [&] { if constexpr (FP64) return A.d12; else return A.f12; }();
+    const KRows<R> d34 = [&] { if constexpr (FP64) return A.d34; else return A.f34; }();
     const int lane = threadIdx.x & 31;
+    KEnt<R>* ring = &ring_all[threadIdx.x >> 5][0][0];
     const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
-    const double thr_dp = A.mixed ? (double) A.thredp : 0.0;
-    long nq = 0, nq32 = 0;
+    const double thr_lo = (double) A.thr_lo, thr_hi = (double) A.thr_hi;   // (float -> double exact)
+    long nq = 0;
     for (;;) {
         int task = 0;
         if (lane == 0) task = (int) atomicAdd(A.queue, 1u);
@@ -114,103 +113,181 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
         const KTask T = A.tasks[task];
         const int i2 = T.i2, i4 = T.i4;
         const double dmax = T.dmax;
-        KGeom g;
-        const double e2 = A.b2.e[i2], e4 = A.b4.e[i4];
-        g.Bx = A.b2.x[i2]; g.By = A.b2.y[i2]; g.Bz = A.b2.z[i2];
-        g.Dx = A.b4.x[i4]; g.Dy = A.b4.y[i4]; g.Dz = A.b4.z[i4];
+        const bool flip = A.flip && i2 != i4;
+        // per-task float thresholds on the bound product (exactly the double screens)
+        const float tlo = float_threshold(thr_lo, dmax);
+        const float thi = float_threshold(thr_hi, dmax);
+        // centre difference R2 - R4 (pair data are relative to these centres)
+        const R dRx = (R) (A.b2.x[i2] - A.b4.x[i4]);
+        const R dRy = (R) (A.b2.y[i2] - A.b4.y[i4]);
+        const R dRz = (R) (A.b2.z[i2] - A.b4.z[i4]);
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
-        double Dblk[N2 * N4];
-        float Dblk32[N2 * N4];
+        R Dblk[N2 * N4];
 #pragma unroll
         for (int a = 0; a < N2; ++a)
 #pragma unroll
-            for (int b = 0; b < N4; ++b) {
-                Dblk[a * N4 + b] = A.Dc[(long) (c2 + a) * A.ld4 + c4 + b];
-                Dblk32[a * N4 + b] = (float) Dblk[a * N4 + b];
-            }
+            for (int b = 0; b < N4; ++b) Dblk[a * N4 + b] = (R) A.Dc[(long) (c2 + a) * A.ld4 + c4 + b];
         const int s12 = A.r12s[i2], n12 = A.r12l[i2];
         const int s34 = A.r34s[i4], n34 = A.r34l[i4];
-        const float b34_0 = A.b34[s34];
-        for (int k1 = 0; k1 < n12; ++k1) {
-            const float b12 = A.b12[s12 + k1];
-            if (b12 < thre12) break;
-            if ((double) (b12 * b34_0) * dmax < (double) A.thresp) break;
-            const double kab12 = A.kab12[s12 + k1], e1 = A.e12[s12 + k1];
-            g.Ax = A.x12[s12 + k1]; g.Ay = A.y12[s12 + k1]; g.Az = A.z12[s12 + k1];
-            const int c1 = A.cart12[s12 + k1];
-            g.p = e1 + e2;
-            g.ip = 1.0 / g.p;
-            g.Px = (e1 * g.Ax + e2 * g.Bx) * g.ip;
-            g.Py = (e1 * g.Ay + e2 * g.By) * g.ip;
-            g.Pz = (e1 * g.Az + e2 * g.Bz) * g.ip;
-            for (int k3 = lane; k3 < n34; k3 += 32) {
-                const float b34 = A.b34[s34 + k3];
-                if (b34 < thre34) break;
-                const double est = (double) (b12 * b34) * dmax;
-                if (est < (double) A.thresp) break;
-                const double e3 = A.e34[s34 + k3];
-                g.Cx = A.x34[s34 + k3]; g.Cy = A.y34[s34 + k3]; g.Cz = A.z34[s34 + k3];
-                const int c3 = A.cart34[s34 + k3];
-                g.kab = kab12 * A.kab34[s34 + k3];
-                g.q = e3 + e4;
-                g.iq = 1.0 / g.q;
-                g.Qx = (e3 * g.Cx + e4 * g.Dx) * g.iq;
-                g.Qy = (e3 * g.Cy + e4 * g.Dy) * g.iq;
-                g.Qz = (e3 * g.Cz + e4 * g.Dz) * g.iq;
-                double KV[N1 * N3];
-                if (est >= thr_dp) {
+        const float b12_max = A.b12[s12];   // first segment's first entry: the row maximum
+
+        for (int cs = 0; cs < n34; cs += 32) {
+            const int k3 = s34 + cs + lane;
+            bool v3 = cs + lane < n34;
+            float b34 = 0.0f;
+            R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
+            int c3 = 0;
+            if (v3) {
+                b34 = A.b34[k3];
+                v3 = b34 >= thre34;
+            }
+            if (v3) {
+                kab34 = d34.kab[k3]; q = d34.p[k3]; iq = d34.ip[k3];
+                Qx = d34.px[k3]; Qy = d34.py[k3]; Qz = d34.pz[k3];
+                Cx = d34.ax[k3]; Cy = d34.ay[k3]; Cz = d34.az[k3];
+                c3 = A.cart34[k3];
+            } else {
+                b34 = 0.0f;
+            }
+            float bmax34 = b34;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
+            if (bmax34 == 0.0f || b12_max * bmax34 < tlo) continue;
+            const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
+            // ket side of PQ: (Q - R4) with the task's centre shift folded in
+            const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
+
+            double acc[N1 * N3];
+#pragma unroll
+            for (int t = 0; t < N1 * N3; ++t) acc[t] = 0.0;
+            bool any = false;
+            int prev_c1 = -1;
+            stage_ent(ring, d12, A.b12, A.cart12, s12, 0, n12, lane);
+            cp_async_commit();
+            bool stop = false;
+            for (int kb = 0; kb < n12 && !stop; kb += 32) {
+                const KEnt<R>* cur = ring + ((kb >> 5) & 1) * 32;
+                if (kb + 32 < n12) stage_ent(ring + (((kb >> 5) + 1) & 1) * 32, d12, A.b12, A.cart12, s12, kb + 32, n12, lane);
+                cp_async_commit();
+                cp_async_wait<1>();
+                __syncwarp();
+                const int kend = min(32, n12 - kb);
+                for (int j = 0; j < kend; ++j) {
+                    const float b12 = cur[j].b;
+                    const int c1 = cur[j].c;
+                    if (c1 != prev_c1) {
+                        if (any) {
+#pragma unroll
+                            for (int a = 0; a < N1; ++a)
+#pragma unroll
+                                for (int c = 0; c < N3; ++c) {
+                                    atomicAdd(&A.Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[a * N3 + c]);
+                                    if (flip) atomicAdd(&A.Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[a * N3 + c]);
+                                    acc[a * N3 + c] = 0.0;
+                                }
+                            any = false;
+                        }
+                        prev_c1 = c1;
+                        // segments are ordered by their largest bound: nothing later passes
+                        if (b12 < thre12 || b12 * bmax34 < tlo) {
+                            stop = true;
+                            break;
+                        }
+                    } else if (b12 < thre12 || b12 * bmax34 < tlo) {
+                        continue;   // rest of this segment
+                    }
+                    const float est = b12 * b34;
+                    const bool pass = v3 && est >= tlo && est < thi;
+                    if (!__any_sync(0xffffffffu, pass)) continue;
+                    if (!pass) continue;
+                    const R kab12 = cur[j].kab, p = cur[j].p, ip = cur[j].ip;
+                    const R Px = cur[j].px, Py = cur[j].py, Pz = cur[j].pz;
+                    const R Ax = cur[j].ax, Ay = cur[j].ay, Az = cur[j].az;
                     ++nq;
+                    any = true;
+                    // PQ = (P - R2) - (Q - R4) + (R2 - R4)
+                    const R PQx = Px + Sx, PQy = Py + Sy, PQz = Pz + Sz;
+                    const R PAx = Px - Ax, PAy = Py - Ay, PAz = Pz - Az;
+                    const R RR = PQx * PQx + PQy * PQy + PQz * PQz;
+                    const R rs = drsqrt(p + q);
+                    const R ipq = rs * rs;
+                    const R rho = p * q * ipq;
+                    // kab fields hold K_ab / p per pair
+                    const R pref = (R) kTwoPi52K * (kab12 * kab34) * rs;
+                    R KV[N1 * N3];
 #pragma unroll
-                    for (int t = 0; t < N1 * N3; ++t) KV[t] = 0.0;
-                    k_quartet64<L1, L2, L3, L4>(A, tab, g, Dblk, KV);
-                } else {
-                    ++nq32;
-                    float KV32[N1 * N3];
+                    for (int t = 0; t < N1 * N3; ++t) KV[t] = R(0);
+                    for (int tm = 0; tm < A.nterm; ++tm) {
+                        R d2 = R(1), f = (R) A.alpha[tm] * pref;
+                        if (A.omega[tm] != -1.0) {
+                            const R w2 = (R) (A.omega[tm] * A.omega[tm]);
+                            d2 = w2 / (rho + w2);
+                            f *= sqrt(d2);
+                        }
+                        R t2[NR], w[NR];
+                        rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
 #pragma unroll
-                    for (int t = 0; t < N1 * N3; ++t) KV32[t] = 0.0f;
-                    k_quartet32<L1, L2, L3, L4>(A, tab32, g, Dblk32, KV32);
+                        for (int r = 0; r < NR; ++r) {
+                            const R u = t2[r] * d2 * ipq;
+                            const R qu = q * u, pu = p * u;
+                            kq_dispatch<L1, L2, L3, L4>(PAx - qu * PQx, PAy - qu * PQy, PAz - qu * PQz,
+                                                        QCx + pu * PQx, QCy + pu * PQy, QCz + pu * PQz,
+                                                        R(0.5) * u, R(0.5) * ip * (R(1) - qu),
+                                                        R(0.5) * iq * (R(1) - pu), Ax, Ay, Az, Cx, Cy, Cz,
+                                                        f * w[r], Dblk, KV);
+                        }
+                    }
 #pragma unroll
-                    for (int t = 0; t < N1 * N3; ++t) KV[t] = (double) KV32[t];
+                    for (int t = 0; t < N1 * N3; ++t) acc[t] += (double) KV[t];
                 }
+                __syncwarp();   // the next chunk's prefetch refills this slot
+            }
+            cp_async_wait<0>();
+            __syncwarp();
+            if (any) {
 #pragma unroll
                 for (int a = 0; a < N1; ++a)
 #pragma unroll
                     for (int c = 0; c < N3; ++c) {
-                        const double v = KV[a * N3 + c];
-                        atomicAdd(&A.Kc[(long) (c1 + a) * A.ld3 + c3 + c], v);
-                        if (A.flip && i2 != i4) atomicAdd(&A.Kc[(long) (c3 + c) * A.ld3 + c1 + a], v);
+                        atomicAdd(&A.Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[a * N3 + c]);
+                        if (flip) atomicAdd(&A.Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[a * N3 + c]);
                     }
             }
         }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        nq += __shfl_xor_sync(0xffffffffu, nq, o);
-        nq32 += __shfl_xor_sync(0xffffffffu, nq32, o);
-    }
-    if (lane == 0) {
-        if (nq) atomicAdd(A.qcount, (unsigned long long) nq);
-        if (nq32) atomicAdd(A.qcount32, (unsigned long long) nq32);
-    }
+    for (int o = 16; o > 0; o >>= 1) nq += __shfl_xor_sync(0xffffffffu, nq, o);
+    if (lane == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
 }
 
 template <int L1, int L2, int L3, int L4>
-void launch_k(Context* ctx, const KArgs& A, long cap)
+void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
 {
     if (cap == 0) return;
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
-    size_t smem = (size_t) 2 * NR * A.nbin * 8 * (sizeof(double) + sizeof(float));
-    static bool attr_set = false;
-    if (!attr_set) {
-        LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int) smem));
-        attr_set = true;
-    }
     long want = (cap + kKWarps - 1) / kKWarps;
-    unsigned grid = (unsigned) std::min<long>(want, 148L * 16);
-    k_exchange<L1, L2, L3, L4><<<grid, kKThreads, smem, ctx->stream>>>(A);
+    int per_sm = ctx->tune.k_ctas_per_sm[fp32 ? 1 : 0][L1][L2][L3][L4];
+    unsigned grid = (unsigned) std::min<long>(want, (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
+    if (!fp32) {
+        size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(double);
+        static bool attr = false;
+        if (!attr) {
+            LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+            attr = true;
+        }
+        k_exchange<L1, L2, L3, L4, double><<<grid, kKThreads, smem, ctx->stream>>>(A);
+    } else {
+        size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(float);
+        static bool attr = false;
+        if (!attr) {
+            LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+            attr = true;
+        }
+        k_exchange<L1, L2, L3, L4, float><<<grid, kKThreads, smem, ctx->stream>>>(A);
+    }
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
 }
-
 
 } // namespace lsjk

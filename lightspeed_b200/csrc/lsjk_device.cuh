@@ -76,19 +76,55 @@ __device__ __forceinline__ bool stage_bulk(void* smem_dst, const void* gsrc, uns
 }
 
 // Horner evaluation of the 8-coefficient per-bin polynomial.
-template <typename R>
-__device__ __forceinline__ R horner8(const R* __restrict__ c, R x)
+// Degree-7 polynomial from 8 coefficients. The coefficient blocks of the
+// quadrature tables start on 32-byte (float) / 64-byte (double) boundaries,
+// so they are fetched with 16-byte vector loads.
+__device__ __forceinline__ float horner8(const float* __restrict__ c, float x)
 {
-    R f = c[7];
-    f = fma(f, x, c[6]);
-    f = fma(f, x, c[5]);
-    f = fma(f, x, c[4]);
-    f = fma(f, x, c[3]);
-    f = fma(f, x, c[2]);
-    f = fma(f, x, c[1]);
-    f = fma(f, x, c[0]);
+    const float4 lo = reinterpret_cast<const float4*>(c)[0];
+    const float4 hi = reinterpret_cast<const float4*>(c)[1];
+    float f = hi.w;
+    f = fmaf(f, x, hi.z);
+    f = fmaf(f, x, hi.y);
+    f = fmaf(f, x, hi.x);
+    f = fmaf(f, x, lo.w);
+    f = fmaf(f, x, lo.z);
+    f = fmaf(f, x, lo.y);
+    f = fmaf(f, x, lo.x);
     return f;
 }
+__device__ __forceinline__ double horner8(const double* __restrict__ c, double x)
+{
+    const double2 c01 = reinterpret_cast<const double2*>(c)[0];
+    const double2 c23 = reinterpret_cast<const double2*>(c)[1];
+    const double2 c45 = reinterpret_cast<const double2*>(c)[2];
+    const double2 c67 = reinterpret_cast<const double2*>(c)[3];
+    double f = c67.y;
+    f = fma(f, x, c67.x);
+    f = fma(f, x, c45.y);
+    f = fma(f, x, c45.x);
+    f = fma(f, x, c23.y);
+    f = fma(f, x, c23.x);
+    f = fma(f, x, c01.y);
+    f = fma(f, x, c01.x);
+    return f;
+}
+
+// Ampere-style asynchronous global -> shared copies of 4 / 8 bytes (one
+// thread each), grouped with commit/wait.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ double dexp(double x) { return exp(x); }
 __device__ __forceinline__ float dexp(float x) { return __expf(x); }

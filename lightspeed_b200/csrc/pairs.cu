@@ -162,6 +162,7 @@ __global__ void k_kinv_entries(const int* __restrict__ p1, const int* __restrict
     }
 }
 
+// pass A key: bound desc, partner asc
 __global__ void k_kinv_key1(const KEnt* __restrict__ e, long n, unsigned long long* __restrict__ key,
                             int* __restrict__ val)
 {
@@ -171,19 +172,41 @@ __global__ void k_kinv_key1(const KEnt* __restrict__ e, long n, unsigned long lo
     val[k] = (int) k;
 }
 
+// pass B key: (class, indexed, partner cartIdx) -- the cartIdx names the contracted shell
 __global__ void k_kinv_key2(const KEnt* __restrict__ e, const int* __restrict__ perm, long n,
-                            unsigned* __restrict__ key)
+                            const int* __restrict__ pcart, unsigned long long* __restrict__ key)
 {
     long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
     if (k >= n) return;
     const KEnt& t = e[perm[k]];
-    key[k] = ((unsigned) t.cls << 16) | (unsigned) t.idx;
+    key[k] = ((unsigned long long) t.cls << 48) | ((unsigned long long) t.idx << 32) | (unsigned) pcart[t.part];
+}
+
+// pass C key: (class, indexed, segment max bound desc); the segment max is the
+// bound of the segment's first entry after pass B.
+__global__ void k_kinv_key3(const KEnt* __restrict__ e, const int* __restrict__ perm,
+                            const unsigned long long* __restrict__ key2s, long n,
+                            unsigned long long* __restrict__ key)
+{
+    long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    long h = k;
+    while (h > 0 && key2s[h - 1] == key2s[k]) --h;   // segments are short (<= shell length)
+    const KEnt& t = e[perm[k]];
+    const KEnt& head = e[perm[h]];
+    key[k] = ((unsigned long long) t.cls << 48) | ((unsigned long long) t.idx << 32) |
+             (unsigned long long) (~__float_as_uint(head.b));
 }
 
 __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ perm, long n,
-                            BasisView bidx, BasisView bpart, double* __restrict__ kab,
-                            double* __restrict__ pe, double* __restrict__ px, double* __restrict__ py,
-                            double* __restrict__ pz, int* __restrict__ pcart, float* __restrict__ pb,
+                            BasisView bidx, BasisView bpart, KInvData* __restrict__ out_unused,
+                            double* __restrict__ kab, double* __restrict__ pp, double* __restrict__ ipp,
+                            double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
+                            double* __restrict__ ax, double* __restrict__ ay, double* __restrict__ az,
+                            float* __restrict__ kab32, float* __restrict__ pp32, float* __restrict__ ipp32,
+                            float* __restrict__ px32, float* __restrict__ py32, float* __restrict__ pz32,
+                            float* __restrict__ ax32, float* __restrict__ ay32, float* __restrict__ az32,
+                            int* __restrict__ pcart, float* __restrict__ pb,
                             int* __restrict__ rstart, int* __restrict__ rlen, int nrow)
 {
     long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
@@ -191,13 +214,16 @@ __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ 
     const KEnt& t = e[perm[k]];
     int i = t.idx, j = t.part;
     double ei = bidx.e[i], ej = bpart.e[j];
-    double dx = bidx.x[i] - bpart.x[j], dy = bidx.y[i] - bpart.y[j], dz = bidx.z[i] - bpart.z[j];
+    double Ax = bpart.x[j] - bidx.x[i], Ay = bpart.y[j] - bidx.y[i], Az = bpart.z[j] - bidx.z[i];
+    double p = ei + ej, ip = 1.0 / p;
     // K_ab = c_a c_b exp(-e_a e_b / (e_a + e_b) |AB|^2)  (kvec.cpp:66-70)
-    kab[k] = bidx.c[i] * bpart.c[j] * exp(-ei * ej / (ei + ej) * (dx * dx + dy * dy + dz * dz));
-    pe[k] = ej;
-    px[k] = bpart.x[j];
-    py[k] = bpart.y[j];
-    pz[k] = bpart.z[j];
+    double K = bidx.c[i] * bpart.c[j] * exp(-ei * ej * ip * (Ax * Ax + Ay * Ay + Az * Az));
+    double Px = ej * Ax * ip, Py = ej * Ay * ip, Pz = ej * Az * ip;   // P - R_i
+    kab[k] = K * ip; pp[k] = p; ipp[k] = ip;   // K_ab / p: the pair's share of the ERI prefactor
+    px[k] = Px; py[k] = Py; pz[k] = Pz; ax[k] = Ax; ay[k] = Ay; az[k] = Az;
+    kab32[k] = (float) (K * ip); pp32[k] = (float) p; ipp32[k] = (float) ip;
+    px32[k] = (float) Px; py32[k] = (float) Py; pz32[k] = (float) Pz;
+    ax32[k] = (float) Ax; ay32[k] = (float) Ay; az32[k] = (float) Az;
     pcart[k] = bpart.cart[j];
     pb[k] = t.b;
     long r = (long) t.cls * nrow + i;
@@ -334,15 +360,8 @@ void build_kinv(Context* ctx, PairList* pl)
             pl->kinv[a][b].row_start.alloc(nrow);
             pl->kinv[a][b].row_len.alloc(nrow);
             pl->kinv[a][b].nent = 0;
-            if (nrow) {
-                LSJK_CUDA(cudaMemsetAsync(pl->kinv[a][b].row_start.p, 0, sizeof(int) * nrow, s));
-                LSJK_CUDA(cudaMemsetAsync(pl->kinv[a][b].row_len.p, 0, sizeof(int) * nrow, s));
-            }
         }
-    kd.nent = cap;
-    kd.kab.alloc(cap); kd.pe.alloc(cap); kd.px.alloc(cap); kd.py.alloc(cap); kd.pz.alloc(cap);
-    kd.pcart.alloc(cap); kd.pbound.alloc(cap);
-    if (n == 0) { pl->kinv_built = true; return; }
+    if (n == 0) { kd.nent = 0; pl->kinv_built = true; return; }
     KEnt* ent = take<KEnt>(ctx, cap);
     unsigned long long* cnt = take<unsigned long long>(ctx, 1);
     LSJK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
@@ -353,24 +372,36 @@ void build_kinv(Context* ctx, PairList* pl)
     LSJK_CUDA(cudaStreamSynchronize(s));
     long m = (long) hn;
     kd.nent = m;
+    kd.kab.alloc(m); kd.p.alloc(m); kd.ip.alloc(m); kd.px.alloc(m); kd.py.alloc(m); kd.pz.alloc(m);
+    kd.ax.alloc(m); kd.ay.alloc(m); kd.az.alloc(m);
+    kd.kab32.alloc(m); kd.p32.alloc(m); kd.ip32.alloc(m); kd.px32.alloc(m); kd.py32.alloc(m);
+    kd.pz32.alloc(m); kd.ax32.alloc(m); kd.ay32.alloc(m); kd.az32.alloc(m);
+    kd.pcart.alloc(m); kd.pbound.alloc(m);
     unsigned long long* ka = take<unsigned long long>(ctx, m);
     unsigned long long* kas = take<unsigned long long>(ctx, m);
     int* va = take<int>(ctx, m);
     int* pa = take<int>(ctx, m);
     k_kinv_key1<<<nblk(m, 256), 256, 0, s>>>(ent, m, ka, va);
     radix_sort_pairs(ctx, ka, kas, va, pa, m, 48);
-    unsigned* kb = take<unsigned>(ctx, m);
-    unsigned* kbs = take<unsigned>(ctx, m);
+    unsigned long long* kb = take<unsigned long long>(ctx, m);
+    unsigned long long* kbs = take<unsigned long long>(ctx, m);
+    int* pb2 = take<int>(ctx, m);
+    k_kinv_key2<<<nblk(m, 256), 256, 0, s>>>(ent, pa, m, bpart->dcart.p, kb);
+    radix_sort_pairs(ctx, kb, kbs, pa, pb2, m, 52);
+    unsigned long long* kc = take<unsigned long long>(ctx, m);
+    unsigned long long* kcs = take<unsigned long long>(ctx, m);
     int* perm = take<int>(ctx, m);
-    k_kinv_key2<<<nblk(m, 256), 256, 0, s>>>(ent, pa, m, kb);
-    radix_sort_pairs(ctx, kb, kbs, pa, perm, m, 32);
+    k_kinv_key3<<<nblk(m, 256), 256, 0, s>>>(ent, pb2, kbs, m, kc);
+    radix_sort_pairs(ctx, kc, kcs, pb2, perm, m, 52);
     // row tables live in one [class][row] block per class
     int* rstart = take<int>(ctx, (long) kNL * kNL * nrow);
     int* rlen = take<int>(ctx, (long) kNL * kNL * nrow);
     LSJK_CUDA(cudaMemsetAsync(rstart, 0, sizeof(int) * kNL * kNL * nrow, s));
     LSJK_CUDA(cudaMemsetAsync(rlen, 0, sizeof(int) * kNL * kNL * nrow, s));
-    k_kinv_fill<<<nblk(m, 256), 256, 0, s>>>(ent, perm, m, bidx->view(), bpart->view(), kd.kab.p, kd.pe.p,
-                                            kd.px.p, kd.py.p, kd.pz.p, kd.pcart.p, kd.pbound.p, rstart,
+    k_kinv_fill<<<nblk(m, 256), 256, 0, s>>>(ent, perm, m, bidx->view(), bpart->view(), nullptr, kd.kab.p, kd.p.p,
+                                            kd.ip.p, kd.px.p, kd.py.p, kd.pz.p, kd.ax.p, kd.ay.p, kd.az.p,
+                                            kd.kab32.p, kd.p32.p, kd.ip32.p, kd.px32.p, kd.py32.p, kd.pz32.p,
+                                            kd.ax32.p, kd.ay32.p, kd.az32.p, kd.pcart.p, kd.pbound.p, rstart,
                                             rlen, nrow);
     LSJK_CUDA(cudaGetLastError());
     for (int a = 0; a < kNL; ++a)
@@ -383,7 +414,7 @@ void build_kinv(Context* ctx, PairList* pl)
         }
     LSJK_CUDA(cudaStreamSynchronize(s));
     pl->kinv_built = true;
-    ctx->stats.kernel_launches += 12;
+    ctx->stats.kernel_launches += 16;
 }
 
 } // namespace lsjk
