@@ -161,6 +161,26 @@ int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, con
                          const double* const* D24_dev, int D24symm, float thresp, float thredp,
                          double* const* K13_dev);
 
+/* J12_dev += J[D34_dev] for one density (device pointers, like
+ * lsjk_coulomb_device), allocating no device memory. No counterpart in the
+ * reference: it is for callers that may not call cudaMalloc/cudaFree while
+ * they run -- a host framework that owns all of the GPU's memory and forbids
+ * allocation after start-up, or a latency-bound loop that cannot take the
+ * device-wide synchronisation an allocation or free can cause. Every
+ * intermediate buffer of the build comes from one static device array of
+ * LSJK_NOALLOC_SCRATCH_BYTES that each GPU loading this library holds until
+ * the process exits; a build that needs more is rejected with LSJK_ENOMEM
+ * (and a message naming the limit) before anything is written to J12_dev.
+ * The first call on a device looks up the array's device address (make that
+ * first call before any stream capture). All calls on a device share the
+ * array, which keeps the previous call's contents (the build clears what must
+ * start at zero), so calls whose GPU work overlaps -- on different streams or
+ * contexts of the same device -- race. */
+#define LSJK_NOALLOC_SCRATCH_BYTES (32u << 20)
+int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                                const lsjk_pairlist* pl12, const lsjk_pairlist* pl34,
+                                const double* D34_dev, float thresp, float thredp, double* J12_dev);
+
 /* ---- CUDA graphs: capture the builds issued through the *_device entry
  * points between lsjk_graph_begin and lsjk_graph_end on the context stream,
  * then replay them with one lsjk_graph_launch (an SCF iteration's J+K as one

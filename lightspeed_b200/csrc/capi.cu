@@ -1,6 +1,8 @@
 // extern "C" entry points of liblsjk.so (declared in include/lsjk.h).
 #include <algorithm>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "engine.cuh"
@@ -597,3 +599,108 @@ int lsjk_graph_destroy(lsjk_graph* graph)
 }
 
 } // extern "C"
+
+// ---- J build without device allocation -------------------------------------
+//
+// Some callers may not allocate device memory while they run: a host framework
+// that hands out all of the GPU's memory itself and forbids cudaMalloc after
+// start-up, or a latency-bound loop that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree can cause. lsjk_coulomb_device_noalloc
+// serves them: every intermediate buffer of the J build (Cartesian D and J,
+// ket records, sort keys and sort workspace, bra accumulators, counters) is
+// carved from the fixed array below instead of the context's growable scratch.
+//
+// The array is a file-scope __device__ object, so every GPU that loads this
+// library holds its LSJK_NOALLOC_SCRATCH_BYTES until the process exits. All
+// calls on a device share it and it keeps the last call's contents; the build
+// clears what must start at zero (counters, accumulators) on every call. Two
+// calls whose work overlaps on the GPU (different streams or contexts on the
+// same device) race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LSJK_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+// Device address of g_noalloc_scratch, looked up once per device. In host
+// code the name g_noalloc_scratch is only a host-side stand-in for the device
+// object; a kernel given it would fault (or, where the GPU can reach host
+// memory, silently use the wrong memory), so kernels get this address.
+char* noalloc_scratch_address(int device)
+{
+    static std::mutex mu;
+    static std::vector<char*> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (device < 0) throw lsjk::Error(LSJK_EINVAL, "noalloc: bad device");
+    if ((int) addr.size() <= device) addr.resize(device + 1, nullptr);
+    if (!addr[device]) {
+        void* p = nullptr;
+        // the caller made `device` current (set_device)
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            throw lsjk::Error(LSJK_ECUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        addr[device] = static_cast<char*>(p);
+    }
+    return addr[device];
+}
+
+// Points the context's scratch allocator at the static array for the lifetime
+// of this object and restores the context's own blocks afterwards (also when
+// the build throws). With scratch_fixed set, a request that does not fit
+// raises LSJK_ENOMEM instead of growing.
+struct StaticScratch {
+    lsjk::Context* ctx;
+    std::vector<std::unique_ptr<lsjk::DBuf<char>>> saved;
+    StaticScratch(lsjk::Context* c, char* base) : ctx(c)
+    {
+        saved.swap(ctx->scratch);
+        ctx->scratch.emplace_back(new lsjk::DBuf<char>());
+        ctx->scratch.back()->p = base;    // not owned: never freed
+        ctx->scratch.back()->n = LSJK_NOALLOC_SCRATCH_BYTES;
+        ctx->scratch_used = 0;
+        ctx->scratch_fixed = true;
+    }
+    ~StaticScratch()
+    {
+        ctx->scratch.back()->p = nullptr;
+        ctx->scratch.back()->n = 0;
+        ctx->scratch.swap(saved);
+        ctx->scratch_used = 0;
+        ctx->scratch_fixed = false;
+    }
+};
+
+} // namespace
+
+extern "C" int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                                           const lsjk_pairlist* pl12, const lsjk_pairlist* pl34,
+                                           const double* D34_dev, float thresp, float thredp, double* J12_dev)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34 || !D34_dev || !J12_dev) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        check_lmax(&pl12->p);
+        check_lmax(&pl34->p);
+        // the Cartesian D and J alone must fit; the rest is checked as the
+        // build takes it, always before the first write to J12
+        const size_t need = ((sizeof(double) * pl34->p.b1->ncart * pl34->p.b2->ncart + 255) & ~size_t(255)) +
+                            ((sizeof(double) * pl12->p.b1->ncart * pl12->p.b2->ncart + 255) & ~size_t(255));
+        if (need > LSJK_NOALLOC_SCRATCH_BYTES)
+            throw lsjk::Error(LSJK_ENOMEM, "lsjk_coulomb_device_noalloc: the basis is too large for the " +
+                                               std::to_string(LSJK_NOALLOC_SCRATCH_BYTES >> 20) +
+                                               " MiB static scratch; use lsjk_coulomb_device");
+        char* base = noalloc_scratch_address(c->device);
+        StaticScratch arena(c, base);
+        const double* d[1] = {D34_dev};
+        double* j[1] = {J12_dev};
+        try {
+            coulomb_group(c, ew, &pl12->p, &pl34->p, d, j, 1, thresp, thredp);
+        } catch (const lsjk::Error& e) {
+            if (e.code == LSJK_ENOMEM)
+                throw lsjk::Error(LSJK_ENOMEM, "lsjk_coulomb_device_noalloc: this J build needs more than the " +
+                                                   std::to_string(LSJK_NOALLOC_SCRATCH_BYTES >> 20) +
+                                                   " MiB static scratch; use lsjk_coulomb_device");
+            throw;
+        }
+    });
+}

@@ -184,6 +184,7 @@ struct Context {
     // scratch buffers reused across calls (grown on demand)
     std::vector<std::unique_ptr<DBuf<char>>> scratch;
     size_t scratch_used = 0;
+    bool scratch_fixed = false;     // scratch is a caller-independent fixed block: never grow
     char* scratch_take(size_t bytes);
     void scratch_reset() { scratch_used = 0; }
     int smem_optin = 0;
@@ -208,6 +209,7 @@ inline char* Context::scratch_take(size_t bytes)
         }
         used += blk->n;
     }
+    if (scratch_fixed) throw Error(LSJK_ENOMEM, "fixed scratch block exhausted");
     size_t sz = std::max(bytes, size_t(64) << 20);
     scratch.emplace_back(new DBuf<char>());
     scratch.back()->alloc(sz);
