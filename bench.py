@@ -41,6 +41,14 @@ def parse():
     ap.add_argument("--carbons", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-maxiter", type=int, default=60)
+    ap.add_argument("--workload", default="alkane", choices=["alkane", "batched", "guess", "many"],
+                    help="alkane: the headline C40H82 J+K step; batched: 64 response-like densities "
+                         "of a 32-water cluster per step (one line per operator and precision); guess: "
+                         "train the learned SCF guess and time SCFs from it against SAD")
+    ap.add_argument("--molecules", type=int, default=512, help="many: number of water clusters")
+    ap.add_argument("--train-clusters", type=int, default=1000)
+    ap.add_argument("--test-clusters", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--profile-step", action="store_true",
                     help="after set-up and warm-up, run one FP64 J+K step between cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off) and exit")
@@ -195,8 +203,9 @@ def run_ours(args):
     # converged density (FP64 J/K), the state an SCF iteration sees
     ls.set_precision(ls.PREC_FP64)
     t0 = time.time()
+    from lightspeed_b200.sad import SAD
     scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    E_scf = scf.compute(maxiter=args.scf_maxiter, g_conv=1e-5)
+    E_scf = scf.compute(D0=SAD(ls, "cc-pvdz").density(mol, bas), maxiter=args.scf_maxiter, g_conv=1e-5)
     t_scf = time.time() - t0
     D = scf.D
     pl = scf.pairs
@@ -352,7 +361,7 @@ def run_ours(args):
             "thre_pq": THRE, "thresp": THRE, "thredp": THREDP, "operator": "1/r",
             "l2": "flushed between steps (256 MiB write outside the timed events)",
             "parallelism": "replicas" if world > 1 else "single-gpu", "scf_iterations": len(scf.trace),
-            "scf_energy": E_scf, "scf_seconds": t_scf},
+            "scf_energy": E_scf, "scf_converged": bool(scf.converged), "scf_guess": "SAD", "scf_seconds": t_scf},
         "fp64": {"ms_per_iter": ms64 / args.steps, "quartets_per_s": fp64_qps, "ms_k": msk64 / args.steps,
                  "quartets": q64, "gpu_launches_per_step": launches_fp64 / max(args.steps, 1)},
         "mixed": {"ms_per_iter": msmx / args.steps, "quartets_per_s": mixed_qps, "ms_k": mskmx / args.steps,
@@ -375,10 +384,316 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """64 non-symmetric densities through one batched J+K step.
+
+    32 H2O (seed 0) in 6-31G* (608 functions), Schwarz 1e-12; densities
+    D_k = A_k B_k^T with A_k, B_k 608 x 10 seeded Gaussian factors made
+    S-orthonormal (the shape of TDA/CIS trial vectors), symmetric pair list,
+    D24symm off. Operators: bare Coulomb and erf-attenuated (omega = 0.3).
+    Per operator and precision: one step = J and K for all 64 densities
+    through the device entry points (J in launches of 4 densities), captured
+    once as a CUDA graph and replayed; the direct (uncaptured) time is
+    reported beside it. Mixed results are compared with FP64 elementwise."""
+    rank, world, local = dist_info()
+    import torch
+    torch.cuda.set_device(local)
+    import lightspeed_b200 as ls
+    from lightspeed_b200.geometry import water_cluster
+    thre = 1.0e-12
+    mol = water_cluster(32, seed=0)
+    bas = ls.Basis.from_gbs_file(mol, "6-31gs")
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, thre)
+    S = ls.IntBox.overlap(res, pl).np.copy()
+    nao = bas.nao
+    ndens, rank_k = 64, 10
+    rng = np.random.default_rng(0)
+    def s_orth(X):
+        M = X.T @ S @ X
+        mw, mU = np.linalg.eigh(M)
+        return X @ ((mU / np.sqrt(mw)) @ mU.T)
+
+    Ds = []
+    for _ in range(ndens):
+        A = s_orth(rng.standard_normal((nao, rank_k)))
+        B = s_orth(rng.standard_normal((nao, rank_k)))
+        Ds.append(A @ B.T)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ls.stream_handle(), device=dev)
+    Dd = torch.tensor(np.stack(Ds), dtype=torch.float64, device=dev)
+    Jd = torch.zeros_like(Dd)
+    Kd = torch.zeros_like(Dd)
+    dptr = [Dd[k].data_ptr() for k in range(ndens)]
+    jptr = [Jd[k].data_ptr() for k in range(ndens)]
+    kptr = [Kd[k].data_ptr() for k in range(ndens)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    results = {}
+    ref = {}
+    clocks = Clocks(local)
+    clocks.start()
+    for opname, (scales, omegas) in (("coulomb", ([1.0], [-1.0])), ("erf_omega0.3", ([1.0], [0.3]))):
+        ew = ls.Ewald(scales, omegas)
+        for prec, mode, thredp in (("fp64", ls.PREC_FP64, thre), ("mixed", ls.PREC_MIXED, THREDP)):
+            ls.set_precision(mode)
+
+            def step():
+                ls.coulomb_device(ew, pl, pl, dptr, jptr, thre, thredp)
+                ls.exchange_device(ew, pl, pl, dptr, False, kptr, thre, thredp)
+
+            for _ in range(args.warmup):
+                with torch.cuda.stream(stream):
+                    Jd.zero_()
+                    Kd.zero_()
+                step()
+            torch.cuda.synchronize()
+            ls.reset_stats()
+            with torch.cuda.stream(stream):
+                Jd.zero_()
+                Kd.zero_()
+            step()
+            torch.cuda.synchronize()
+            st = ls.stats()
+            if prec == "fp64":
+                ref[opname] = (Jd.clone(), Kd.clone())
+                err = None
+            else:
+                J64, K64 = ref[opname]
+                err = {"max_abs_dJ": (Jd - J64).abs().max().item(), "max_abs_dK": (Kd - K64).abs().max().item()}
+            ls.graph_begin()
+            step()
+            g = ls.graph_end()
+
+            def timed(fn):
+                tot = 0.0
+                for _ in range(args.steps):
+                    with torch.cuda.stream(stream):
+                        flush.zero_()
+                        Jd.zero_()
+                        Kd.zero_()
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        fn()
+                        e1.record(stream)
+                    e1.synchronize()
+                    tot += e0.elapsed_time(e1)
+                return tot / args.steps
+
+            ms_graph = timed(g.launch)
+            ms_direct = timed(step)
+            del g
+            q = st["j_quartets"] + st["k_quartets"]
+            results["%s/%s" % (opname, prec)] = {
+                "ms_per_step": ms_graph, "ms_per_step_direct": ms_direct, "quartets": q,
+                "quartets_fp32": st["quartets_fp32"], "quartets_per_s": q / (ms_graph * 1e-3),
+                "ms_per_density": ms_graph / ndens, "error_vs_fp64": err,
+                "gpu_launches_per_step": st["kernel_launches"]}
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if rank != 0:
+        return 0
+    head = results["coulomb/mixed"]
+    line = {
+        "metric": "batched J+K, 64 densities: ms per step and quartets/s (mixed vs FP64)",
+        "value": head["quartets_per_s"], "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (mixed)", "data": "synthetic",
+        "config": {"workload": "32 H2O (seed 0) / 6-31G*, 64 non-symmetric rank-10 densities, J+K",
+                   "nao": nao, "thresp": thre, "thredp": THREDP, "graph": "one CUDA graph per step",
+                   "l2": "flushed between steps (256 MiB write outside the timed events)"},
+        "results": results, "gpu_launches": int(head["gpu_launches_per_step"] * args.steps), "clocks": clk}
+    print(json.dumps(line))
+    return 0
+
+
+def run_guess(args):
+    """Learned SCF guess against SAD on seeded water clusters (6-31G*, FP64 J/K).
+
+    Training: converged densities (orbital gradient 1e-6, from SAD) of
+    `--train-clusters` seeded clusters of 4-16 H2O with +-0.05 A bond and
+    +-5 degree angle noise (seeds 0..), features and local-frame targets per
+    atom pair, `--epochs` epochs of the BF16 network. Evaluation: held-out
+    clusters of 20-24 H2O (seeds 100000..), each converged to 1e-8 from SAD
+    and from the learned guess (SAD fallback on 1e-3 trace/idempotency
+    error); wall time includes building the guess. `value` = total SAD SCF
+    wall time / total learned-guess SCF wall time."""
+    rank, world, local = dist_info()
+    import torch
+    torch.cuda.set_device(local)
+    import lightspeed_b200 as ls
+    from lightspeed_b200 import guess as g
+    from lightspeed_b200.sad import SAD
+    if rank != 0:
+        return 0
+    ls.set_precision(ls.PREC_FP64)
+    sad = SAD(ls, "6-31gs")
+    rng = np.random.default_rng(0)
+    train = [(int(rng.integers(4, 17)), s) for s in range(args.train_clusters)]
+    test = [(int(rng.integers(20, 25)), 100000 + s) for s in range(args.test_clusters)]
+    t0 = time.time()
+    X, Y, W = g.training_set(ls, train, sad)
+    t_data = time.time() - t0
+    net = g.MLP(ls, seed=0)
+    t0 = time.time()
+    hist = net.fit(X, Y, W, epochs=args.epochs, batch=4096, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.time() - t0
+    # warm the SCF path once so neither arm pays first-call costs
+    g.compare_guesses(ls, g.LearnedGuess(net, sad), [(test[0][0], test[0][1] + 50000)])
+    rows = g.compare_guesses(ls, g.LearnedGuess(net, sad), test)
+    t_sad = sum(r["sad"]["seconds"] for r in rows)
+    t_mlp = sum(r["mlp"]["seconds"] for r in rows)
+    line = {
+        "metric": "SCF wall time, learned guess vs SAD (water clusters of 20-24 H2O, 6-31G*, to 1e-8)",
+        "value": t_sad / t_mlp, "unit": "x (SAD time / learned-guess time)", "n_gpus": 1,
+        "higher_is_better": True, "data": "synthetic", "dtype": "bf16 network, f64 SCF",
+        "config": {"workload": "learned SCF guess", "train_clusters": len(train), "train_sizes": "4-16 H2O",
+                   "test_clusters": len(test), "test_sizes": "20-24 H2O", "noise": "+-0.05 A, +-5 deg",
+                   "train_pairs": int(X.shape[0]), "epochs": args.epochs, "network": "3 x 256 SiLU, bf16"},
+        "seconds_training_data": t_data, "seconds_training": t_train,
+        "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
+        "sad": {"iterations_mean": float(np.mean([r["sad"]["iterations"] for r in rows])), "seconds": t_sad},
+        "mlp": {"iterations_mean": float(np.mean([r["mlp"]["iterations"] for r in rows])), "seconds": t_mlp,
+                "fallbacks": sum(r["mlp"]["source"] != "mlp" for r in rows)},
+        "max_abs_dE_Eh": max(abs(r["dE"]) for r in rows),
+        "all_converged": all(r["sad"]["converged"] and r["mlp"]["converged"] for r in rows),
+        "rows": rows,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_many(args):
+    """Many-molecule batch: `--molecules` seeded water clusters of 1-12 H2O
+    (sizes from default_rng(0), cluster m from seed m), 6-31G*, FP64 J/K,
+    each converged from SAD to an orbital gradient of 1e-8. The SCFs run in
+    lockstep; per iteration the difference densities of all unconverged
+    molecules go to the device in one copy, and their J and K builds run
+    either (a) as a sequential per-molecule loop of device calls, or (b) as
+    one CUDA graph holding every molecule's builds (captured once per active
+    set, replayed while the set is unchanged), then J and K come back in one
+    copy. Reported per mode: molecules/s over the whole run, quartets/s over
+    the J/K phases (device events), and the wall time split."""
+    rank, world, local = dist_info()
+    import torch
+    torch.cuda.set_device(local)
+    import lightspeed_b200 as ls
+    from lightspeed_b200.geometry import water_cluster
+    from lightspeed_b200.sad import SAD
+    from lightspeed_b200.scf import RHF, SCFStepper
+    if rank != 0:
+        return 0
+    ls.set_precision(ls.PREC_FP64)
+    thre = 1.0e-12
+    sizes = np.random.default_rng(0).integers(1, 13, size=args.molecules)
+    sad = SAD(ls, "6-31gs")
+    t0 = time.time()
+    systems = []
+    for m, n in enumerate(sizes):
+        mol = water_cluster(int(n), seed=m)
+        bas = ls.Basis.from_gbs_file(mol, "6-31gs")
+        systems.append((mol, bas, RHF(ls, mol, bas, thre_pq=thre, thre_sp=thre, thre_dp=thre)))
+    t_setup = time.time() - t0
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ls.stream_handle(), device=dev)
+    ew = ls.Ewald.coulomb()
+    naos = [b.nao for _, b, _ in systems]
+    offs = np.concatenate([[0], np.cumsum([n * n for n in naos])])
+    D_dev = torch.zeros(int(offs[-1]), dtype=torch.float64, device=dev)
+    JK_dev = torch.zeros(2, int(offs[-1]), dtype=torch.float64, device=dev)
+    D_host = torch.zeros(int(offs[-1]), dtype=torch.float64).pin_memory()
+    JK_host = torch.zeros(2, int(offs[-1]), dtype=torch.float64).pin_memory()
+    ptr = lambda t, m: t.data_ptr() + 8 * int(offs[m])
+
+    def builds(active):
+        for m in active:
+            pl = systems[m][2].pairs
+            ls.coulomb_device(ew, pl, pl, [ptr(D_dev, m)], [ptr(JK_dev[0], m)], thre, thre)
+            ls.exchange_device(ew, pl, pl, [ptr(D_dev, m)], True, [ptr(JK_dev[1], m)], thre, thre)
+
+    results = {}
+    energies = {}
+    for mode in ("sequential", "graph"):
+        steppers = [SCFStepper(r, sad.density(mol, bas), g_conv=1.0e-8) for mol, bas, r in systems]
+        active = list(range(len(systems)))
+        graph, graph_set = None, None
+        t_start = time.time()
+        gpu_ms, iters, q = 0.0, 0, 0
+        ls.reset_stats()
+        Dh = D_host.numpy()
+        JKh = JK_host.numpy()
+        while active and iters < 100:
+            iters += 1
+            for m in active:
+                Dh[offs[m]:offs[m + 1]] = steppers[m].build_density().ravel()
+            with torch.cuda.stream(stream):
+                D_dev.copy_(D_host, non_blocking=True)
+                JK_dev.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if mode == "graph" and graph is not None and graph_set == active:
+                    graph.launch()
+                    e1.record(stream)
+                else:
+                    builds(active)
+                    e1.record(stream)
+                    if mode == "graph":
+                        # a new active set: these builds ran directly; capture them for the next iterations
+                        graph = None
+                        ls.graph_begin()
+                        builds(active)
+                        graph = ls.graph_end()
+                        graph_set = list(active)
+                JK_host.copy_(JK_dev, non_blocking=True)
+            stream.synchronize()
+            gpu_ms += e0.elapsed_time(e1)
+            nxt = []
+            for m in active:
+                n = naos[m]
+                dJ = JKh[0, offs[m]:offs[m + 1]].reshape(n, n)
+                dK = JKh[1, offs[m]:offs[m + 1]].reshape(n, n)
+                if not steppers[m].update(dJ.copy(), dK.copy()):
+                    nxt.append(m)
+            active = nxt
+        for st in steppers:
+            st.finish()
+        wall = time.time() - t_start
+        stt = ls.stats()
+        q = stt["j_quartets"] + stt["k_quartets"]
+        energies[mode] = np.array([r.E for _, _, r in systems])
+        results[mode] = {"seconds": wall, "molecules_per_s": len(systems) / wall, "lockstep_iterations": iters,
+                         "jk_gpu_seconds": gpu_ms * 1e-3, "quartets": q,
+                         "quartets_per_s": q / max(gpu_ms * 1e-3, 1e-12),
+                         "converged": int(sum(st.converged for st in steppers)),
+                         "gpu_launches": stt["kernel_launches"]}
+        del graph
+    line = {
+        "metric": "many-molecule batch: molecules/s and quartets/s, one CUDA graph per SCF iteration vs "
+                  "a sequential per-molecule GPU loop",
+        "value": results["graph"]["molecules_per_s"], "unit": "molecules/s", "n_gpus": 1,
+        "higher_is_better": True, "data": "synthetic", "dtype": "f64",
+        "config": {"workload": "%d water clusters of 1-12 H2O (sizes from seed 0, cluster m from seed m), 6-31G*, "
+                               "RHF from SAD to 1e-8" % len(systems), "thresp": thre,
+                   "total_functions": int(sum(naos)), "setup_seconds": t_setup},
+        "sequential": results["sequential"], "graph": results["graph"],
+        "speedup_graph_vs_sequential": results["sequential"]["seconds"] / results["graph"]["seconds"],
+        "max_abs_dE_graph_vs_sequential": float(np.max(np.abs(energies["graph"] - energies["sequential"]))),
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "guess":
+        return run_guess(args)
+    if args.workload == "many":
+        return run_many(args)
     return run_ours(args)
 
 

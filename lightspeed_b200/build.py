@@ -63,7 +63,7 @@ def gen_sources(force=False):
 def cuda_units():
     """(object name, source, extra flags) for every translation unit."""
     units = []
-    for name in ("basis", "pairs", "capi", "jbuild", "kbuild"):
+    for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "mlp"):
         units.append((name, os.path.join(CSRC, name + ".cu"), []))
     for lb in range(2 * LMAX + 1):
         units.append(("jinst_%d" % lb, os.path.join(CSRC, "jinst.cu"), ["-DLSJK_LB=%d" % lb]))

@@ -96,19 +96,25 @@ void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairLi
     for (int g = 0; g < ng; ++g) lsjk::cart_to_pure_acc(ctx, b1, b2, Jc[g], Jpure[g]);
 }
 
-void exchange_one(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
-                  const lsjk::PairList* pl34, const double* Dpure, bool d24symm, bool flip_ok,
-                  double* Kpure, float thresp, float thredp)
+// One K build for ng (1..4) densities sharing the quartet integrals, device
+// pointers in and out.
+void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
+                    const lsjk::PairList* pl34, const double* const* Dpure, bool d24symm, bool flip_ok,
+                    double* const* Kpure, int ng, float thresp, float thredp)
 {
     ctx->scratch_reset();
     const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
-    double* Dc = lsjk::take<double>(ctx, (size_t) b2->ncart * b4->ncart);
-    double* Kc = lsjk::take<double>(ctx, (size_t) b1->ncart * b3->ncart);
-    lsjk::pure_to_cart(ctx, b2, b4, Dpure, Dc);
-    LSJK_CUDA(cudaMemsetAsync(Kc, 0, sizeof(double) * b1->ncart * b3->ncart, ctx->stream));
+    double* Dc[lsjk::kJBatchMax];
+    double* Kc[lsjk::kJBatchMax];
+    for (int g = 0; g < ng; ++g) {
+        Dc[g] = lsjk::take<double>(ctx, (size_t) b2->ncart * b4->ncart);
+        Kc[g] = lsjk::take<double>(ctx, (size_t) b1->ncart * b3->ncart);
+        lsjk::pure_to_cart(ctx, b2, b4, Dpure[g], Dc[g]);
+        LSJK_CUDA(cudaMemsetAsync(Kc[g], 0, sizeof(double) * b1->ncart * b3->ncart, ctx->stream));
+    }
     if (!ew.alpha.empty() && pl12->npair && pl34->npair)
-        lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Kc, d24symm, flip_ok, thresp, thredp);
-    lsjk::cart_to_pure_acc(ctx, b1, b3, Kc, Kpure);
+        lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Kc, ng, d24symm, flip_ok, thresp, thredp);
+    for (int g = 0; g < ng; ++g) lsjk::cart_to_pure_acc(ctx, b1, b3, Kc[g], Kpure[g]);
 }
 
 void exchange_prepare(lsjk::Context* ctx, lsjk::PairList* pl12, lsjk::PairList* pl34, int D24symm,
@@ -473,8 +479,9 @@ int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, con
         bool d24 = false, flip = false;
         exchange_prepare(&ctx->c, const_cast<lsjk::PairList*>(&pl12->p), const_cast<lsjk::PairList*>(&pl34->p),
                          D24symm, &d24, &flip);
-        for (int k = 0; k < ndens; ++k)
-            exchange_one(&ctx->c, ew, &pl12->p, &pl34->p, D24[k], d24, flip, K13[k], thresp, thredp);
+        for (int k0 = 0; k0 < ndens; k0 += lsjk::kJBatchMax)
+            exchange_group(&ctx->c, ew, &pl12->p, &pl34->p, D24 + k0, d24, flip, K13 + k0,
+                           std::min(lsjk::kJBatchMax, ndens - k0), thresp, thredp);
     });
 }
 
@@ -533,17 +540,28 @@ int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const doub
                          &d24, &flip);
         const size_t nD = (size_t) pl12->p.b2->nao * pl34->p.b2->nao;
         const size_t nK = (size_t) pl12->p.b1->nao * pl34->p.b1->nao;
+        const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
         lsjk::DBuf<double> dD, dK;
-        dD.alloc(nD);
-        dK.alloc(nK);
-        std::vector<double> hK(nK);
-        for (int k = 0; k < ndens; ++k) {
-            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p, D24[k], sizeof(double) * nD, cudaMemcpyHostToDevice, c->stream));
-            if (nK) LSJK_CUDA(cudaMemsetAsync(dK.p, 0, sizeof(double) * nK, c->stream));
-            exchange_one(c, ew, &pl12->p, &pl34->p, dD.p, d24, flip, dK.p, thresp, thredp);
-            if (nK) LSJK_CUDA(cudaMemcpyAsync(hK.data(), dK.p, sizeof(double) * nK, cudaMemcpyDeviceToHost, c->stream));
+        dD.alloc(nD * G);
+        dK.alloc(nK * G);
+        std::vector<double> hK(nK * G);
+        for (int k0 = 0; k0 < ndens; k0 += G) {
+            const int ng = std::min(G, ndens - k0);
+            const double* dp[lsjk::kJBatchMax];
+            double* kp[lsjk::kJBatchMax];
+            for (int g = 0; g < ng; ++g) {
+                dp[g] = dD.p + g * nD;
+                kp[g] = dK.p + g * nK;
+                if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p + g * nD, D24[k0 + g], sizeof(double) * nD,
+                                                  cudaMemcpyHostToDevice, c->stream));
+            }
+            if (nK) LSJK_CUDA(cudaMemsetAsync(dK.p, 0, sizeof(double) * nK * ng, c->stream));
+            exchange_group(c, ew, &pl12->p, &pl34->p, dp, d24, flip, kp, ng, thresp, thredp);
+            if (nK) LSJK_CUDA(cudaMemcpyAsync(hK.data(), dK.p, sizeof(double) * nK * ng, cudaMemcpyDeviceToHost,
+                                              c->stream));
             check_kernels(c);
-            for (size_t i = 0; i < nK; ++i) K13[k][i] += hK[i];
+            for (int g = 0; g < ng; ++g)
+                for (size_t i = 0; i < nK; ++i) K13[k0 + g][i] += hK[g * nK + i];
         }
     });
 }

@@ -233,15 +233,17 @@ struct Ewald {
     std::vector<double> alpha, omega;   // terms with alpha != 0 and omega != 0
 };
 
-// densities per batched J launch
+// densities per batched J or K build (one quartet loop for all of them)
 constexpr int kJBatchMax = 4;
 
 // J for ng (1..4) densities at once; batched densities share the quartets
 // (screened with the largest |D| of the batch).
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                    const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp);
+// K for ng (1..4) densities sharing one task list (screened with the largest
+// |D24| of the batch) and the quartet integrals.
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                    const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
+                    const double* const* Dcart, double* const* Kcart, int ng, bool d24symm, bool flip_ok,
                     float thresp, float thredp);
 
 } // namespace lsjk

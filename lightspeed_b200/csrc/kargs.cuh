@@ -7,6 +7,7 @@ namespace lsjk {
 
 constexpr int kKThreads = 128;
 constexpr int kKWarps = kKThreads / 32;
+constexpr int kKBatch = 4;        // densities per K build (one task list, screened with their largest |D|)
 
 // One (prim2, prim4) task: the K-invert rows of prim2 (partners 1) and prim4
 // (partners 3) and the largest |D24| over the pair's Cartesian block.
@@ -31,7 +32,7 @@ struct KRows {
 struct KArgs {
     const KTask* tasks;
     const int* ntask;
-    unsigned* queue;
+    unsigned* queue;             // work-queue counters, one per kernel launch of the pass
     const int* r12s;          // rows of prim2 in class (L2 indexed, L1 partner)
     const int* r12l;
     const int* r34s;          // rows of prim4 in class (L4, L3)
@@ -43,10 +44,11 @@ struct KArgs {
     const int* cart34;
     const float* b34;
     BasisView b2, b4;         // indexed primitives (centres, cartIdx)
-    const double* Dc;
+    const double* Dc[kKBatch];   // D24 of each density of the launch (Cartesian, ld4)
     int ld4;
-    double* Kc;
+    double* Kc[kKBatch];         // K13 of each density (Cartesian, ld3)
     int ld3;
+    int ng;                      // densities: launch_k splits them over kernel launches
     int flip;
     // this pass computes quartets with thr_lo <= estimate < thr_hi
     float thr_lo, thr_hi;

@@ -63,7 +63,8 @@ struct TaskGenArgs {
     KRowTables r12, r34;
     const float* pb12;
     const float* pb34;
-    const double* Dc;
+    const double* Dc[kKBatch];
+    int ng;
     int ld4;
     int d24symm;
     float thresp;
@@ -83,9 +84,11 @@ __global__ void k_task_gen(TaskGenArgs A)
     int L2 = A.b2.L[i2], L4 = A.b4.L[i4];
     int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
     int n2 = ncart_of(L2), n4 = ncart_of(L4);
+    // largest |D24| over the pair's block and the batch's densities
     double dmax = 0.0;
-    for (int a = 0; a < n2; ++a)
-        for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[(long) (c2 + a) * A.ld4 + c4 + b]));
+    for (int g = 0; g < A.ng; ++g)
+        for (int a = 0; a < n2; ++a)
+            for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b]));
     for (int L1 = 0; L1 < kNL; ++L1) {
         const int* rl12 = A.r12.len[L2][L1];
         if (!rl12) continue;
@@ -162,9 +165,10 @@ double k_quartet_flops(int L1, int L2, int L3, int L4)
 }
 
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                    const double* Dcart, double* Kcart, bool d24symm, bool flip_ok,
+                    const double* const* Dcart, double* const* Kcart, int ng, bool d24symm, bool flip_ok,
                     float thresp, float thredp)
 {
+    if (ng < 1 || ng > kKBatch) throw Error(LSJK_EINVAL, "exchange_build: 1..4 densities per build");
     cudaStream_t s = ctx->stream;
     const int b1c = pl12->b1->ncart;
     const Basis *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
@@ -172,10 +176,13 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     KScalars* sc = take<KScalars>(ctx, 1);
     LSJK_CUDA(cudaMemsetAsync(sc, 0, sizeof(KScalars), s));
     long nd = (long) pl12->b2->ncart * b4->ncart;
-    if (nd) k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(Dcart, nd, &sc->dmax_bits);
+    for (int g = 0; g < ng && nd; ++g) {
+        k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(Dcart[g], nd, &sc->dmax_bits);
+        ctx->stats.kernel_launches++;
+    }
     k_kscalars<<<1, 1, 0, s>>>(sc, thresp, pl12->max_bound, pl34->max_bound);
     LSJK_CUDA(cudaGetLastError());
-    ctx->stats.kernel_launches += 2;
+    ctx->stats.kernel_launches++;
 
     // per-combo task regions: capacity = prims of L2 in basis2 x prims of L4 in basis4
     int cnt2[kNL] = {0}, cnt4[kNL] = {0};
@@ -192,12 +199,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
     int* ntask = take<int>(ctx, kNCombo);
-    unsigned* queue = take<unsigned>(ctx, 2 * kNCombo);
+    unsigned* queue = take<unsigned>(ctx, 2 * kNCombo * kKBatch);   // per class, pass and launch
     unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
     unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
     const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
     LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
-    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo, s));
+    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo * kKBatch, s));
 
     TaskGenArgs G{};
     G.b2 = b2->view();
@@ -211,7 +218,8 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
         }
     G.pb12 = pl12->kdat.pbound.p;
     G.pb34 = pl34->kdat.pbound.p;
-    G.Dc = Dcart;
+    for (int g = 0; g < ng; ++g) G.Dc[g] = Dcart[g];
+    G.ng = ng;
     G.ld4 = b4->ncart;
     G.d24symm = d24symm ? 1 : 0;
     G.thresp = thresp;
@@ -260,9 +268,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.b34 = d34.pbound.p;
                     A.b2 = b2->view();
                     A.b4 = b4->view();
-                    A.Dc = Dcart;
+                    for (int g = 0; g < ng; ++g) {
+                        A.Dc[g] = Dcart[g];
+                        A.Kc[g] = Kcart[g];
+                    }
+                    A.ng = ng;
                     A.ld4 = b4->ncart;
-                    A.Kc = Kcart;
                     A.ld3 = b3->ncart;
                     A.flip = flip_ok ? 1 : 0;
                     A.sc = sc;
@@ -276,7 +287,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     }
                     const float inf = __builtin_huge_valf();
                     // FP64 pass: estimate >= thredp (mixed) or >= thresp (FP64 mode)
-                    A.queue = queue + c;
+                    A.queue = queue + (long) c * kKBatch;
                     A.thr_lo = mixed ? thredp : thresp;
                     A.thr_hi = inf;
                     A.rys = ctx->rys64.p + kRysOffset[NR];
@@ -287,7 +298,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         // autotuner: time candidate grid sizes on scratch outputs
                         static const int cand[] = {2, 4, 8, 16, 32};
                         KArgs T = X;
-                        T.Kc = take<double>(ctx, (size_t) b1c * b3->ncart);
+                        for (int g = 0; g < X.ng; ++g) T.Kc[g] = take<double>(ctx, (size_t) b1c * b3->ncart);
                         T.qcount = ctx->tune_sink.p;
                         int& slot = ctx->tune.k_ctas_per_sm[fp32 ? 1 : 0][L1][L2][L3][L4];
                         float best = 1e30f;
@@ -296,7 +307,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                             slot = cnd;
                             float ms = 1e30f;
                             for (int rep = 0; rep < 2; ++rep) {
-                                LSJK_CUDA(cudaMemsetAsync(T.queue, 0, sizeof(unsigned), s));
+                                LSJK_CUDA(cudaMemsetAsync(T.queue, 0, sizeof(unsigned) * kKBatch, s));
                                 LSJK_CUDA(cudaEventRecord(ctx->ev0, s));
                                 launch_k1(ctx, T, cap, L1, L2, L3, L4, fp32);
                                 LSJK_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -311,13 +322,13 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                             }
                         }
                         slot = bestc;
-                        LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned), s));
+                        LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned) * kKBatch, s));
                     };
                     if (ctx->tuning) tune(A, false);
                     launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
                     if (mixed) {
                         // FP32 pass: thresp <= estimate < thredp
-                        A.queue = queue + kNCombo + c;
+                        A.queue = queue + (long) (kNCombo + c) * kKBatch;
                         A.thr_lo = thresp;
                         A.thr_hi = thredp;
                         A.rys = ctx->rys32.p + kRysOffset[NR];

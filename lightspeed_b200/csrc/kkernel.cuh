@@ -10,6 +10,8 @@
 // as broadcasts. Partners 1 come grouped by contracted shell, so a lane sums
 // the quartets of one shell segment -- same K13 target block -- in registers
 // and issues one FP64 atomic per element when the segment ends.
+// Up to k_batch densities share a launch: the integrals of a quartet are
+// formed once and contracted with each density's D24 block.
 // Screens (per quartet, exactly the reference's set):
 //   bound12 >= thre12, bound34 >= thre34,
 //   thr_lo <= double(float(bound12*bound34)) * max|D24 block| < thr_hi
@@ -80,8 +82,75 @@ __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const
     cp_async4(&o->c, cart + e);
 }
 
+// Densities per launch for a class: up to kKBatch while the per-density
+// registers (FP64 accumulators and the partial quartet block of N1*N3, the
+// D24 block of N2*N4, counted in 32-bit registers) stay within 64; 1 above.
 template <int L1, int L2, int L3, int L4, typename R>
-__global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
+__host__ __device__ constexpr int k_batch()
+{
+    constexpr int w = sizeof(R) / 4;
+    constexpr int per = ncart_of(L1) * ncart_of(L3) * (2 + w) + ncart_of(L2) * ncart_of(L4) * w;
+    return 4 * per <= 64 ? 4 : (2 * per <= 64 ? 2 : 1);
+}
+
+// One quartet (partner 1 from the staged entry e, partner 3 from registers)
+// contracted with the NG densities' D24 blocks, added to the FP64
+// accumulators. The Rys roots, weights and 1-D integrals are shared by the
+// densities (the NG inlined contractions see identical integral inputs).
+template <int L1, int L2, int L3, int L4, typename R, int NG>
+__device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ tab, R tmax,
+                                          const R* __restrict__ asym_t, const R* __restrict__ asym_w,
+                                          const KEnt<R>& e, R kab34, R q, R iq, R Sx, R Sy, R Sz, R QCx,
+                                          R QCy, R QCz, R Cx, R Cy, R Cz, const R (*Dblk)[ncart_of(L2) * ncart_of(L4)],
+                                          double (*acc)[ncart_of(L1) * ncart_of(L3)])
+{
+    constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
+    constexpr int N1 = ncart_of(L1), N3 = ncart_of(L3);
+    const R p = e.p, ip = e.ip;
+    // PQ = (P - R2) - (Q - R4) + (R2 - R4)
+    const R PQx = e.px + Sx, PQy = e.py + Sy, PQz = e.pz + Sz;
+    const R PAx = e.px - e.ax, PAy = e.py - e.ay, PAz = e.pz - e.az;
+    const R RR = PQx * PQx + PQy * PQy + PQz * PQz;
+    const R rs = drsqrt(p + q);
+    const R ipq = rs * rs;
+    const R rho = p * q * ipq;
+    // kab fields hold K_ab / p per pair
+    const R pref = (R) kTwoPi52K * (e.kab * kab34) * rs;
+    R KV[NG][N1 * N3];
+#pragma unroll
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+        for (int t = 0; t < N1 * N3; ++t) KV[g][t] = R(0);
+    for (int tm = 0; tm < A.nterm; ++tm) {
+        R d2 = R(1), f = (R) A.alpha[tm] * pref;
+        if (A.omega[tm] != -1.0) {
+            const R w2 = (R) (A.omega[tm] * A.omega[tm]);
+            d2 = w2 / (rho + w2);
+            f *= sqrt(d2);
+        }
+        R t2[NR], w[NR];
+        rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const R u = t2[r] * d2 * ipq;
+            const R qu = q * u, pu = p * u;
+            const R c00x = PAx - qu * PQx, c00y = PAy - qu * PQy, c00z = PAz - qu * PQz;
+            const R d00x = QCx + pu * PQx, d00y = QCy + pu * PQy, d00z = QCz + pu * PQz;
+            const R b00 = R(0.5) * u, b10 = R(0.5) * ip * (R(1) - qu), b01 = R(0.5) * iq * (R(1) - pu);
+#pragma unroll
+            for (int g = 0; g < NG; ++g)
+                kq_dispatch<L1, L2, L3, L4>(c00x, c00y, c00z, d00x, d00y, d00z, b00, b10, b01, e.ax, e.ay, e.az,
+                                            Cx, Cy, Cz, f * w[r], Dblk[g], KV[g]);
+        }
+    }
+#pragma unroll
+    for (int g = 0; g < NG; ++g)
+#pragma unroll
+        for (int t = 0; t < N1 * N3; ++t) acc[g][t] += (double) KV[g][t];
+}
+
+template <int L1, int L2, int L3, int L4, typename R, int NG>
+__global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ KArgs A)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
@@ -112,7 +181,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
         if (task >= ntask) break;
         const KTask T = A.tasks[task];
         const int i2 = T.i2, i4 = T.i4;
-        const double dmax = T.dmax;
+        const double dmax = T.dmax;   // largest |D24 block| over the densities of the batch
         const bool flip = A.flip && i2 != i4;
         // per-task float thresholds on the bound product (exactly the double screens)
         const float tlo = float_threshold(thr_lo, dmax);
@@ -122,25 +191,29 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
         const R dRy = (R) (A.b2.y[i2] - A.b4.y[i4]);
         const R dRz = (R) (A.b2.z[i2] - A.b4.z[i4]);
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
-        R Dblk[N2 * N4];
+        R Dblk[NG][N2 * N4];
 #pragma unroll
-        for (int a = 0; a < N2; ++a)
+        for (int g = 0; g < NG; ++g)
 #pragma unroll
-            for (int b = 0; b < N4; ++b) Dblk[a * N4 + b] = (R) A.Dc[(long) (c2 + a) * A.ld4 + c4 + b];
+            for (int a = 0; a < N2; ++a)
+#pragma unroll
+                for (int b = 0; b < N4; ++b)
+                    Dblk[g][a * N4 + b] = (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b];
         const int s12 = A.r12s[i2], n12 = A.r12l[i2];
         const int s34 = A.r34s[i4], n34 = A.r34l[i4];
         const float b12_max = A.b12[s12];   // first segment's first entry: the row maximum
 
         for (int cs = 0; cs < n34; cs += 32) {
+            // partner 3 of this lane: entry cs + lane of the row
             const int k3 = s34 + cs + lane;
             bool v3 = cs + lane < n34;
             float b34 = 0.0f;
-            R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
-            int c3 = 0;
             if (v3) {
                 b34 = A.b34[k3];
                 v3 = b34 >= thre34;
             }
+            R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
+            int c3 = 0;
             if (v3) {
                 kab34 = d34.kab[k3]; q = d34.p[k3]; iq = d34.ip[k3];
                 Qx = d34.px[k3]; Qy = d34.py[k3]; Qz = d34.pz[k3];
@@ -149,19 +222,40 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
             } else {
                 b34 = 0.0f;
             }
+            const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
+            // ket side of PQ: (Q - R4) with the task's centre shift folded in
+            const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
             float bmax34 = b34;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
             if (bmax34 == 0.0f || b12_max * bmax34 < tlo) continue;
-            const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
-            // ket side of PQ: (Q - R4) with the task's centre shift folded in
-            const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
-
-            double acc[N1 * N3];
+            double acc[NG][N1 * N3];
 #pragma unroll
-            for (int t = 0; t < N1 * N3; ++t) acc[t] = 0.0;
+            for (int g = 0; g < NG; ++g)
+#pragma unroll
+                for (int t = 0; t < N1 * N3; ++t) acc[g][t] = 0.0;
             bool any = false;
             int prev_c1 = -1;
+            // flush the finished shell segment of partner 1: one atomic per element and density
+            // (fire-and-forget reductions; a segmented shuffle sum over the lanes of one shell 3
+            // before them measured slower)
+            auto flush = [&]() {
+                if (any) {
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) {
+                        double* Kc = A.Kc[g];
+#pragma unroll
+                        for (int a = 0; a < N1; ++a)
+#pragma unroll
+                            for (int c = 0; c < N3; ++c) {
+                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[g][a * N3 + c]);
+                                if (flip) atomicAdd(&Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[g][a * N3 + c]);
+                                acc[g][a * N3 + c] = 0.0;
+                            }
+                    }
+                }
+                any = false;
+            };
             stage_ent(ring, d12, A.b12, A.cart12, s12, 0, n12, lane);
             cp_async_commit();
             bool stop = false;
@@ -172,21 +266,15 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
                 cp_async_wait<1>();
                 __syncwarp();
                 const int kend = min(32, n12 - kb);
+                // chg bit l: entry l of the chunk starts a new shell segment (l >= 1)
+                const int cl = lane < kend ? cur[lane].c : -1;
+                const int cl_prev = __shfl_up_sync(0xffffffffu, cl, 1);
+                const unsigned chg = __ballot_sync(0xffffffffu, lane >= 1 && lane < kend && cl != cl_prev);
                 for (int j = 0; j < kend; ++j) {
                     const float b12 = cur[j].b;
                     const int c1 = cur[j].c;
                     if (c1 != prev_c1) {
-                        if (any) {
-#pragma unroll
-                            for (int a = 0; a < N1; ++a)
-#pragma unroll
-                                for (int c = 0; c < N3; ++c) {
-                                    atomicAdd(&A.Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[a * N3 + c]);
-                                    if (flip) atomicAdd(&A.Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[a * N3 + c]);
-                                    acc[a * N3 + c] = 0.0;
-                                }
-                            any = false;
-                        }
+                        flush();
                         prev_c1 = c1;
                         // segments are ordered by their largest bound: nothing later passes
                         if (b12 < thre12 || b12 * bmax34 < tlo) {
@@ -194,100 +282,90 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(KArgs A)
                             break;
                         }
                     } else if (b12 < thre12 || b12 * bmax34 < tlo) {
-                        continue;   // rest of this segment
+                        // entries of a segment are ordered by bound: skip the rest of this
+                        // segment within the chunk (to the next segment start, or the chunk end)
+                        const unsigned nxt = j == 31 ? 0u : (chg & ~((2u << j) - 1u));
+                        j = (nxt ? __ffs(nxt) - 1 : kend) - 1;
+                        continue;
                     }
                     const float est = b12 * b34;
                     const bool pass = v3 && est >= tlo && est < thi;
                     if (!__any_sync(0xffffffffu, pass)) continue;
                     if (!pass) continue;
-                    const R kab12 = cur[j].kab, p = cur[j].p, ip = cur[j].ip;
-                    const R Px = cur[j].px, Py = cur[j].py, Pz = cur[j].pz;
-                    const R Ax = cur[j].ax, Ay = cur[j].ay, Az = cur[j].az;
+                    const KEnt<R> e = cur[j];
                     ++nq;
                     any = true;
-                    // PQ = (P - R2) - (Q - R4) + (R2 - R4)
-                    const R PQx = Px + Sx, PQy = Py + Sy, PQz = Pz + Sz;
-                    const R PAx = Px - Ax, PAy = Py - Ay, PAz = Pz - Az;
-                    const R RR = PQx * PQx + PQy * PQy + PQz * PQz;
-                    const R rs = drsqrt(p + q);
-                    const R ipq = rs * rs;
-                    const R rho = p * q * ipq;
-                    // kab fields hold K_ab / p per pair
-                    const R pref = (R) kTwoPi52K * (kab12 * kab34) * rs;
-                    R KV[N1 * N3];
-#pragma unroll
-                    for (int t = 0; t < N1 * N3; ++t) KV[t] = R(0);
-                    for (int tm = 0; tm < A.nterm; ++tm) {
-                        R d2 = R(1), f = (R) A.alpha[tm] * pref;
-                        if (A.omega[tm] != -1.0) {
-                            const R w2 = (R) (A.omega[tm] * A.omega[tm]);
-                            d2 = w2 / (rho + w2);
-                            f *= sqrt(d2);
-                        }
-                        R t2[NR], w[NR];
-                        rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
-#pragma unroll
-                        for (int r = 0; r < NR; ++r) {
-                            const R u = t2[r] * d2 * ipq;
-                            const R qu = q * u, pu = p * u;
-                            kq_dispatch<L1, L2, L3, L4>(PAx - qu * PQx, PAy - qu * PQy, PAz - qu * PQz,
-                                                        QCx + pu * PQx, QCy + pu * PQy, QCz + pu * PQz,
-                                                        R(0.5) * u, R(0.5) * ip * (R(1) - qu),
-                                                        R(0.5) * iq * (R(1) - pu), Ax, Ay, Az, Cx, Cy, Cz,
-                                                        f * w[r], Dblk, KV);
-                        }
-                    }
-#pragma unroll
-                    for (int t = 0; t < N1 * N3; ++t) acc[t] += (double) KV[t];
+                    k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy, Sz, QCx,
+                                                     QCy, QCz, Cx, Cy, Cz, Dblk, acc);
                 }
                 __syncwarp();   // the next chunk's prefetch refills this slot
             }
             cp_async_wait<0>();
             __syncwarp();
-            if (any) {
-#pragma unroll
-                for (int a = 0; a < N1; ++a)
-#pragma unroll
-                    for (int c = 0; c < N3; ++c) {
-                        atomicAdd(&A.Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[a * N3 + c]);
-                        if (flip) atomicAdd(&A.Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[a * N3 + c]);
-                    }
-            }
+            flush();
         }
     }
     for (int o = 16; o > 0; o >>= 1) nq += __shfl_xor_sync(0xffffffffu, nq, o);
     if (lane == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
 }
 
+template <int L1, int L2, int L3, int L4, typename R, int NG>
+void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
+{
+    constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
+    const size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(R);
+    static bool attr = false;
+    if (!attr) {
+        LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, R, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int) smem));
+        attr = true;
+    }
+    k_exchange<L1, L2, L3, L4, R, NG><<<grid, kKThreads, smem, ctx->stream>>>(A);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+}
+
+// One class, one precision pass, A.ng densities: launches of k_batch densities
+// while they last, then single-density launches. Each launch takes its own
+// work-queue counter (A.queue[launch index], zeroed by the caller).
 template <int L1, int L2, int L3, int L4>
 void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
 {
-    if (cap == 0) return;
-    constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
+    if (cap == 0 || A.ng < 1) return;
     long want = (cap + kKWarps - 1) / kKWarps;
     int per_sm = ctx->tune.k_ctas_per_sm[fp32 ? 1 : 0][L1][L2][L3][L4];
     unsigned grid = (unsigned) std::min<long>(want, (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
-    if (!fp32) {
-        size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(double);
-        static bool attr = false;
-        if (!attr) {
-            LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, double>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-            attr = true;
+    KArgs B = A;
+    int g0 = 0, launch = 0;
+    while (g0 < A.ng) {
+        for (int g = 0; g < kKBatch; ++g) {
+            B.Dc[g] = g0 + g < A.ng ? A.Dc[g0 + g] : nullptr;
+            B.Kc[g] = g0 + g < A.ng ? A.Kc[g0 + g] : nullptr;
         }
-        k_exchange<L1, L2, L3, L4, double><<<grid, kKThreads, smem, ctx->stream>>>(A);
-    } else {
-        size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(float);
-        static bool attr = false;
-        if (!attr) {
-            LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, float>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-            attr = true;
+        B.queue = A.queue + launch;
+        int used;
+        if (fp32) {
+            constexpr int NGf = k_batch<L1, L2, L3, L4, float>();
+            if (NGf > 1 && A.ng - g0 >= NGf) {
+                launch_k_one<L1, L2, L3, L4, float, NGf>(ctx, B, grid);
+                used = NGf;
+            } else {
+                launch_k_one<L1, L2, L3, L4, float, 1>(ctx, B, grid);
+                used = 1;
+            }
+        } else {
+            constexpr int NGd = k_batch<L1, L2, L3, L4, double>();
+            if (NGd > 1 && A.ng - g0 >= NGd) {
+                launch_k_one<L1, L2, L3, L4, double, NGd>(ctx, B, grid);
+                used = NGd;
+            } else {
+                launch_k_one<L1, L2, L3, L4, double, 1>(ctx, B, grid);
+                used = 1;
+            }
         }
-        k_exchange<L1, L2, L3, L4, float><<<grid, kKThreads, smem, ctx->stream>>>(A);
+        g0 += used;
+        ++launch;
     }
-    LSJK_CUDA(cudaGetLastError());
-    ctx->stats.kernel_launches++;
 }
 
 } // namespace lsjk

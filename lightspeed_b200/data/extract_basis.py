@@ -12,7 +12,7 @@ import os
 import re
 import sys
 
-NAMES = ["sto-3g", "3-21g", "6-31g", "6-31gs", "6-31gss", "cc-pvdz"]
+NAMES = ["sto-3g", "3-21g", "6-31g", "6-31gs", "6-31gss", "cc-pvdz", "cc-pvdz-minao"]
 KEEP = {"H", "HE", "LI", "BE", "B", "C", "N", "O", "F", "NE"}
 
 

@@ -61,63 +61,116 @@ class RHF:
         return self.density(self.H)[0]
 
     # -- iterations --------------------------------------------------------------
-    def compute(self, D0=None, maxiter=60, g_conv=1.0e-8, e_conv=1.0e-10, ndiis=8, verbose=False):
-        D = self.core_guess() if D0 is None else np.array(D0, copy=True)
-        Dold = np.zeros_like(D)
-        J = np.zeros_like(D)
-        K = np.zeros_like(D)
-        diis_F, diis_E = [], []
-        E_old = 0.0
-        self.trace = []
+    def compute(self, D0=None, maxiter=60, g_conv=1.0e-8, e_conv=None, ndiis=8, verbose=False):
+        """Converge until the orbital gradient (rms, orthogonal basis) is below
+        g_conv on a Fock matrix from a full (not incremental) J/K build: when an
+        incremental build reaches g_conv, the same density is rebuilt in full
+        and tested again, so the final energy carries no accumulated
+        difference-density screening error. e_conv, if given, also bounds the
+        last energy change."""
+        st = SCFStepper(self, D0, g_conv=g_conv, e_conv=e_conv, ndiis=ndiis)
         t_start = time.time()
         for it in range(maxiter):
-            if it % self.incremental_niter == 0:
-                J[...] = 0.0
-                K[...] = 0.0
-                Dold[...] = 0.0
+            dD = st.build_density()
             t0 = time.time()
-            dJ, dK = self.jk(D - Dold)
-            t_jk = time.time() - t0
-            J += dJ
-            K += dK
-            Dold = D.copy()
-            E, F = self.energy(D, J, K)
-            G = F @ D @ self.S - self.S @ D @ F
-            Go = self.X.T @ G @ self.X
-            gnorm = float(np.sqrt(np.mean(Go * Go)))
-            dE = E - E_old
-            E_old = E
-            self.trace.append(dict(iter=it, E=E, dE=dE, gnorm=gnorm, t_jk=t_jk))
+            dJ, dK = self.jk(dD)
+            st.t_jk = time.time() - t0
+            done = st.update(dJ, dK)
             if verbose:
-                print("  %3d %24.16f %11.3e %11.3e %8.3f s" % (it, E, dE, gnorm, t_jk), flush=True)
-            if gnorm < g_conv and abs(dE) < max(e_conv, 1e-14):
+                tr = self.trace[-1]
+                print("  %3d %24.16f %11.3e %11.3e %8.3f s%s" % (it, tr["E"], tr["dE"], tr["gnorm"], st.t_jk,
+                                                                  "" if tr["full"] else " (incr)"), flush=True)
+            if done:
                 break
-            diis_F.append(F.copy())
-            diis_E.append(Go.copy())
-            if len(diis_F) > ndiis:
-                diis_F.pop(0)
-                diis_E.pop(0)
-            n = len(diis_F)
-            B = -np.ones((n + 1, n + 1))
-            B[n, n] = 0.0
-            for a in range(n):
-                for b in range(n):
-                    B[a, b] = np.sum(diis_E[a] * diis_E[b])
-            rhs = np.zeros(n + 1)
-            rhs[n] = -1.0
-            try:
-                c = np.linalg.solve(B, rhs)[:n]
-            except np.linalg.LinAlgError:
-                c = np.zeros(n)
-                c[-1] = 1.0
-            Fd = sum(ci * Fi for ci, Fi in zip(c, diis_F))
-            D = self.density(Fd)[0]
-        self.E = E
-        self.D = D
-        self.J, self.K = J, K
+        st.finish()
         self.wall = time.time() - t_start
-        self.converged = gnorm < g_conv
-        return E
+        return self.E
+
+
+class SCFStepper:
+    """One RHF's iterations as explicit steps, so a driver can build the J/K
+    of many molecules together: build_density() gives the (difference)
+    density to build, update(dJ, dK) consumes the result and returns True once
+    converged. The iteration follows est/rhf.py:583-660: incremental Fock
+    builds with dD = D - D_old and a full rebuild every `incremental_niter`
+    iterations, DIIS on F D S - S D F, convergence confirmed on a full build."""
+
+    def __init__(self, rhf, D0=None, g_conv=1.0e-8, e_conv=None, ndiis=8):
+        self.r = rhf
+        self.D = rhf.core_guess() if D0 is None else np.array(D0, copy=True)
+        self.Dold = np.zeros_like(self.D)
+        self.J = np.zeros_like(self.D)
+        self.K = np.zeros_like(self.D)
+        self.diis_F, self.diis_E = [], []
+        self.E_old = 0.0
+        self.g_conv, self.e_conv, self.ndiis = g_conv, e_conv, ndiis
+        self.force_full = False
+        self.n_full = 0
+        self.full = True
+        self.gnorm = np.inf
+        self.E = None
+        self.t_jk = 0.0
+        self.converged = False
+        rhf.trace = []
+
+    def build_density(self):
+        self.full = self.force_full or self.n_full % self.r.incremental_niter == 0
+        self.force_full = False
+        if self.full:
+            self.n_full = 0
+            self.J[...] = 0.0
+            self.K[...] = 0.0
+            self.Dold[...] = 0.0
+        self.n_full += 1
+        return self.D - self.Dold
+
+    def update(self, dJ, dK):
+        r = self.r
+        self.J += dJ
+        self.K += dK
+        self.Dold = self.D.copy()
+        E, F = r.energy(self.D, self.J, self.K)
+        G = F @ self.D @ r.S - r.S @ self.D @ F
+        Go = r.X.T @ G @ r.X
+        self.gnorm = float(np.sqrt(np.mean(Go * Go)))
+        dE = E - self.E_old
+        self.E_old = E
+        self.E = E
+        r.trace.append(dict(iter=len(r.trace), E=E, dE=dE, gnorm=self.gnorm, t_jk=self.t_jk, full=self.full))
+        if self.gnorm < self.g_conv and (self.e_conv is None or abs(dE) < self.e_conv):
+            if self.full:
+                self.converged = True
+                return True
+            self.force_full = True     # confirm on a full build of the same density
+            return False
+        self.diis_F.append(F.copy())
+        self.diis_E.append(Go.copy())
+        if len(self.diis_F) > self.ndiis:
+            self.diis_F.pop(0)
+            self.diis_E.pop(0)
+        n = len(self.diis_F)
+        B = -np.ones((n + 1, n + 1))
+        B[n, n] = 0.0
+        for a in range(n):
+            for b in range(n):
+                B[a, b] = np.sum(self.diis_E[a] * self.diis_E[b])
+        rhs = np.zeros(n + 1)
+        rhs[n] = -1.0
+        try:
+            c = np.linalg.solve(B, rhs)[:n]
+        except np.linalg.LinAlgError:
+            c = np.zeros(n)
+            c[-1] = 1.0
+        Fd = sum(ci * Fi for ci, Fi in zip(c, self.diis_F))
+        self.D = r.density(Fd)[0]
+        return False
+
+    def finish(self):
+        r = self.r
+        r.E = self.E
+        r.D = self.D
+        r.J, r.K = self.J, self.K
+        r.converged = self.converged
 
 
 def loewdin_density(S, nocc, seed):

@@ -12,14 +12,17 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_symbols():
-    src = open(os.path.join(ROOT, "include", "lsjk.h")).read()
-    return sorted(set(re.findall(r"\b(lsjk_[a-z_]+)\s*\(", src)))
+    names = set()
+    for h in ("lsjk.h", "lsmlp.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"\b(ls(?:jk|mlp)_[a-z0-9_]+)\s*\(", src))
+    return sorted(names)
 
 
 def test_header_symbols_exported(ls):
     lib = ctypes.CDLL(ls.LIB_PATH)
     names = declared_symbols()
-    assert len(names) >= 18
+    assert len(names) >= 26
     for n in names:
         assert hasattr(lib, n), n
 

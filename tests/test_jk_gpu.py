@@ -127,6 +127,30 @@ def test_water8_vs_oracle_fixture(ls, golden_dir):
     assert np.max(abs(K.np - z["K"])) < 1e-10
 
 
+def test_propane_ccpvdz_vs_reference(ls):
+    """C3H8 / cc-pVDZ (spherical d on carbon, long contracted s shells): J and K
+    of a SAD-like symmetric density elementwise 1e-10 against the reference
+    CPU IntBox, symmetric and non-symmetric K."""
+    from lightspeed_b200.geometry import alkane
+    if not ref.available():
+        pytest.skip("reference CPU IntBox not built")
+    bas = ls.Basis.from_gbs_file(alkane(3), "cc-pvdz")
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((bas.nao, 13)) / np.sqrt(bas.nao)
+    D = X @ X.T
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    J = ls.IntBox.coulomb(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.array(D), 1e-14, 1e-14).np
+    assert np.max(abs(J - ref.coulomb(rp, rp, D, 1e-14, 1e-14))) < 1e-10
+    K = ls.IntBox.exchange(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-14).np
+    assert np.max(abs(K - ref.exchange(rp, rp, D, True, 1e-14, 1e-14))) < 1e-10
+    Dn = D + 0.05 * np.triu(X @ X[::-1].T)
+    Kn = ls.IntBox.exchange(res, ls.Ewald.coulomb(), pl, pl, ls.Tensor.array(Dn), False, 1e-14, 1e-14).np
+    assert np.max(abs(Kn - ref.exchange(rp, rp, Dn, False, 1e-14, 1e-14))) < 1e-10
+
+
 def test_d24symm_requires_equivalent_bases(ls, golden_dir):
     b1 = _h2o(ls, golden_dir, "sto-3g")
     b2 = _h2o(ls, golden_dir, "6-31gs")
