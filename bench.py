@@ -205,7 +205,7 @@ def run_ours(args):
     t0 = time.time()
     from lightspeed_b200.sad import SAD
     scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    E_scf = scf.compute(D0=SAD(ls, "cc-pvdz").density(mol, bas), maxiter=args.scf_maxiter, g_conv=1e-5)
+    E_scf = scf.compute(D0=SAD(ls, "cc-pvdz").density(mol, bas), maxiter=args.scf_maxiter, g_conv=1e-6)
     t_scf = time.time() - t0
     D = scf.D
     pl = scf.pairs
@@ -486,7 +486,9 @@ def run_batched(args):
             q = st["j_quartets"] + st["k_quartets"]
             results["%s/%s" % (opname, prec)] = {
                 "ms_per_step": ms_graph, "ms_per_step_direct": ms_direct, "quartets": q,
+                "density_quartets": 4 * q,   # every launch serves 4 densities (64 = 16 groups of 4)
                 "quartets_fp32": st["quartets_fp32"], "quartets_per_s": q / (ms_graph * 1e-3),
+                "density_quartets_per_s": 4 * q / (ms_graph * 1e-3),
                 "ms_per_density": ms_graph / ndens, "error_vs_fp64": err,
                 "gpu_launches_per_step": st["kernel_launches"]}
     torch.cuda.synchronize()
@@ -516,7 +518,8 @@ def run_guess(args):
     atom pair, `--epochs` epochs of the BF16 network. Evaluation: held-out
     clusters of 20-24 H2O (seeds 100000..), each converged to 1e-8 from SAD
     and from the learned guess (SAD fallback on 1e-3 trace/idempotency
-    error); wall time includes building the guess. `value` = total SAD SCF
+    error); wall time includes building the guess (fastest of two runs per
+    cluster and arm). `value` = total SAD SCF
     wall time / total learned-guess SCF wall time."""
     rank, world, local = dist_info()
     import torch
@@ -541,7 +544,7 @@ def run_guess(args):
     t_train = time.time() - t0
     # warm the SCF path once so neither arm pays first-call costs
     g.compare_guesses(ls, g.LearnedGuess(net, sad), [(test[0][0], test[0][1] + 50000)])
-    rows = g.compare_guesses(ls, g.LearnedGuess(net, sad), test)
+    rows = g.compare_guesses(ls, g.LearnedGuess(net, sad), test, repeats=2)
     t_sad = sum(r["sad"]["seconds"] for r in rows)
     t_mlp = sum(r["mlp"]["seconds"] for r in rows)
     line = {

@@ -8,7 +8,40 @@
 #include "engine.cuh"
 #include "lsjk_device.cuh"
 
-struct lsjk_context { lsjk::Context c; };
+// Page-locked host staging for the host-pointer entry points (grow-only).
+struct PinnedBuf {
+    double* p = nullptr;
+    size_t n = 0;
+    PinnedBuf() = default;
+    PinnedBuf(const PinnedBuf&) = delete;
+    PinnedBuf& operator=(const PinnedBuf&) = delete;
+    ~PinnedBuf() { if (p) cudaFreeHost(p); }
+    double* ensure(size_t count)
+    {
+        if (count > n) {
+            if (p) cudaFreeHost(p);
+            p = nullptr;
+            n = 0;
+            LSJK_CUDA(cudaMallocHost((void**) &p, sizeof(double) * count));
+            n = count;
+        }
+        return p;
+    }
+};
+
+// The context plus the device and pinned host buffers the host-pointer entry
+// points (lsjk_coulomb, lsjk_exchange) stage D and J/K through; both grow to
+// the largest call and are reused, so repeated calls allocate nothing.
+struct lsjk_context {
+    lsjk::Context c;
+    lsjk::DBuf<double> io_dev;
+    PinnedBuf io_host;
+    double* dev(size_t count)
+    {
+        if (count > io_dev.n) io_dev.alloc(count);
+        return io_dev.p;
+    }
+};
 struct lsjk_basis { lsjk::Basis b; };
 struct lsjk_pairlist { lsjk::PairList p; };
 struct lsjk_graph {
@@ -500,24 +533,23 @@ int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const doubl
         const size_t nD = (size_t) pl34->p.b1->nao * pl34->p.b2->nao;
         const size_t nJ = (size_t) pl12->p.b1->nao * pl12->p.b2->nao;
         const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
-        lsjk::DBuf<double> dD, dJ;
-        dD.alloc(nD * G);
-        dJ.alloc(nJ * G);
-        std::vector<double> hJ(nJ * G);
+        double* dD = ctx->dev((nD + nJ) * G);
+        double* dJ = dD + nD * G;
+        double* hD = ctx->io_host.ensure((nD + nJ) * G);
+        double* hJ = hD + nD * G;
         for (int k0 = 0; k0 < ndens; k0 += G) {
             const int ng = std::min(G, ndens - k0);
             const double* dp[lsjk::kJBatchMax];
             double* jp[lsjk::kJBatchMax];
             for (int g = 0; g < ng; ++g) {
-                dp[g] = dD.p + g * nD;
-                jp[g] = dJ.p + g * nJ;
-                if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p + g * nD, D34[k0 + g], sizeof(double) * nD,
-                                                  cudaMemcpyHostToDevice, c->stream));
+                dp[g] = dD + g * nD;
+                jp[g] = dJ + g * nJ;
+                if (nD) std::memcpy(hD + g * nD, D34[k0 + g], sizeof(double) * nD);
             }
-            if (nJ) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * nJ * ng, c->stream));
+            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD, hD, sizeof(double) * nD * ng, cudaMemcpyHostToDevice, c->stream));
+            if (nJ) LSJK_CUDA(cudaMemsetAsync(dJ, 0, sizeof(double) * nJ * ng, c->stream));
             coulomb_group(c, ew, &pl12->p, &pl34->p, dp, jp, ng, thresp, thredp);
-            if (nJ) LSJK_CUDA(cudaMemcpyAsync(hJ.data(), dJ.p, sizeof(double) * nJ * ng, cudaMemcpyDeviceToHost,
-                                              c->stream));
+            if (nJ) LSJK_CUDA(cudaMemcpyAsync(hJ, dJ, sizeof(double) * nJ * ng, cudaMemcpyDeviceToHost, c->stream));
             check_kernels(c);
             for (int g = 0; g < ng; ++g)
                 for (size_t i = 0; i < nJ; ++i) J12[k0 + g][i] += hJ[g * nJ + i];
@@ -541,24 +573,23 @@ int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const doub
         const size_t nD = (size_t) pl12->p.b2->nao * pl34->p.b2->nao;
         const size_t nK = (size_t) pl12->p.b1->nao * pl34->p.b1->nao;
         const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
-        lsjk::DBuf<double> dD, dK;
-        dD.alloc(nD * G);
-        dK.alloc(nK * G);
-        std::vector<double> hK(nK * G);
+        double* dD = ctx->dev((nD + nK) * G);
+        double* dK = dD + nD * G;
+        double* hD = ctx->io_host.ensure((nD + nK) * G);
+        double* hK = hD + nD * G;
         for (int k0 = 0; k0 < ndens; k0 += G) {
             const int ng = std::min(G, ndens - k0);
             const double* dp[lsjk::kJBatchMax];
             double* kp[lsjk::kJBatchMax];
             for (int g = 0; g < ng; ++g) {
-                dp[g] = dD.p + g * nD;
-                kp[g] = dK.p + g * nK;
-                if (nD) LSJK_CUDA(cudaMemcpyAsync(dD.p + g * nD, D24[k0 + g], sizeof(double) * nD,
-                                                  cudaMemcpyHostToDevice, c->stream));
+                dp[g] = dD + g * nD;
+                kp[g] = dK + g * nK;
+                if (nD) std::memcpy(hD + g * nD, D24[k0 + g], sizeof(double) * nD);
             }
-            if (nK) LSJK_CUDA(cudaMemsetAsync(dK.p, 0, sizeof(double) * nK * ng, c->stream));
+            if (nD) LSJK_CUDA(cudaMemcpyAsync(dD, hD, sizeof(double) * nD * ng, cudaMemcpyHostToDevice, c->stream));
+            if (nK) LSJK_CUDA(cudaMemsetAsync(dK, 0, sizeof(double) * nK * ng, c->stream));
             exchange_group(c, ew, &pl12->p, &pl34->p, dp, d24, flip, kp, ng, thresp, thredp);
-            if (nK) LSJK_CUDA(cudaMemcpyAsync(hK.data(), dK.p, sizeof(double) * nK * ng, cudaMemcpyDeviceToHost,
-                                              c->stream));
+            if (nK) LSJK_CUDA(cudaMemcpyAsync(hK, dK, sizeof(double) * nK * ng, cudaMemcpyDeviceToHost, c->stream));
             check_kernels(c);
             for (int g = 0; g < ng; ++g)
                 for (size_t i = 0; i < nK; ++i) K13[k0 + g][i] += hK[g * nK + i];

@@ -155,7 +155,8 @@ struct PairList {
     JBraClass jb[kNHerm];
     // K-invert rows: [L_indexed][L_partner]
     KInvClass kinv[kNL][kNL];
-    KInvData kdat;
+    KInvData kdat;     // rows grouped by contracted shell (segments): the partner-1 side of K
+    KInvData kdat_b;   // the same rows, entries by bound only: the partner-3 side of K
     bool kinv_built = false;
 };
 

@@ -252,8 +252,8 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.r12l = pl12->kinv[L2][L1].row_len.p;
                     A.r34s = pl34->kinv[L4][L3].row_start.p;
                     A.r34l = pl34->kinv[L4][L3].row_len.p;
-                    const KInvData& d12 = pl12->kdat;
-                    const KInvData& d34 = pl34->kdat;
+                    const KInvData& d12 = pl12->kdat;     // partner 1: shell segments
+                    const KInvData& d34 = pl34->kdat_b;   // partner 3: by bound
                     A.d12 = KRows<double>{d12.kab.p, d12.p.p, d12.ip.p, d12.px.p, d12.py.p, d12.pz.p,
                                           d12.ax.p, d12.ay.p, d12.az.p};
                     A.d34 = KRows<double>{d34.kab.p, d34.p.p, d34.ip.p, d34.px.p, d34.py.p, d34.pz.p,

@@ -3,8 +3,9 @@
 // generated quartet header so the classes build in parallel.
 //
 // Work unit: one (prim2, prim4) task, taken by a warp from a device queue.
-// The 32 lanes own 32 consecutive partners 3 of prim4 (their pair data stay
-// in registers for the whole task); the warp walks the partners 1 of prim2,
+// The 32 lanes own 32 consecutive partners 3 of prim4, taken from a copy of
+// the rows ordered by bound alone (their pair data stay in registers while
+// the chunk is processed); the warp walks the partners 1 of prim2,
 // which are staged 32 at a time into a per-warp shared-memory ring by
 // cp.async (the next 32 are in flight while the current 32 are used) and read
 // as broadcasts. Partners 1 come grouped by contracted shell, so a lane sums
@@ -160,7 +161,9 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     __shared__ __align__(8) uint64_t mbar;
     __shared__ KEnt<R> ring_all[kKWarps][2][32];
     const int ntask = *A.ntask;
-    if (ntask == 0) return;
+    // the grid is sized for the class's task capacity; CTAs whose warps cannot
+    // get a task leave before staging the quadrature table
+    if ((long) blockIdx.x * kKWarps >= ntask) return;
     const unsigned bytes = (unsigned) (2 * NR * A.nbin * 8 * sizeof(R));
     if (!stage_bulk(tab, A.rys, bytes, &mbar, A.status)) return;
     const R* asym_t = static_cast<const R*>(A.asym_t);
@@ -228,7 +231,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
             float bmax34 = b34;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
-            if (bmax34 == 0.0f || b12_max * bmax34 < tlo) continue;
+            // partners 3 come by bound: no later chunk passes either
+            if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
             double acc[NG][N1 * N3];
 #pragma unroll
             for (int g = 0; g < NG; ++g)

@@ -182,6 +182,17 @@ __global__ void k_kinv_key2(const KEnt* __restrict__ e, const int* __restrict__ 
     key[k] = ((unsigned long long) t.cls << 48) | ((unsigned long long) t.idx << 32) | (unsigned) pcart[t.part];
 }
 
+// row key (class, indexed): a stable pass over the bound order gives each row
+// its entries by bound alone (the partner-3 copy of the rows)
+__global__ void k_kinv_keyrow(const KEnt* __restrict__ e, const int* __restrict__ perm, long n,
+                              unsigned long long* __restrict__ key)
+{
+    long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const KEnt& t = e[perm[k]];
+    key[k] = ((unsigned long long) t.cls << 32) | (unsigned) t.idx;
+}
+
 // pass C key: (class, indexed, segment max bound desc); the segment max is the
 // bound of the segment's first entry after pass B.
 __global__ void k_kinv_key3(const KEnt* __restrict__ e, const int* __restrict__ perm,
@@ -383,6 +394,11 @@ void build_kinv(Context* ctx, PairList* pl)
     int* pa = take<int>(ctx, m);
     k_kinv_key1<<<nblk(m, 256), 256, 0, s>>>(ent, m, ka, va);
     radix_sort_pairs(ctx, ka, kas, va, pa, m, 48);
+    unsigned long long* kr = take<unsigned long long>(ctx, m);
+    unsigned long long* krs = take<unsigned long long>(ctx, m);
+    int* perm_b = take<int>(ctx, m);
+    k_kinv_keyrow<<<nblk(m, 256), 256, 0, s>>>(ent, pa, m, kr);
+    radix_sort_pairs(ctx, kr, krs, pa, perm_b, m, 36);
     unsigned long long* kb = take<unsigned long long>(ctx, m);
     unsigned long long* kbs = take<unsigned long long>(ctx, m);
     int* pb2 = take<int>(ctx, m);
@@ -404,6 +420,24 @@ void build_kinv(Context* ctx, PairList* pl)
                                             kd.ax32.p, kd.ay32.p, kd.az32.p, kd.pcart.p, kd.pbound.p, rstart,
                                             rlen, nrow);
     LSJK_CUDA(cudaGetLastError());
+    // the bound-ordered copy (same rows, so the same row tables)
+    KInvData& kb_ = pl->kdat_b;
+    kb_.nent = m;
+    kb_.kab.alloc(m); kb_.p.alloc(m); kb_.ip.alloc(m); kb_.px.alloc(m); kb_.py.alloc(m); kb_.pz.alloc(m);
+    kb_.ax.alloc(m); kb_.ay.alloc(m); kb_.az.alloc(m);
+    kb_.kab32.alloc(m); kb_.p32.alloc(m); kb_.ip32.alloc(m); kb_.px32.alloc(m); kb_.py32.alloc(m);
+    kb_.pz32.alloc(m); kb_.ax32.alloc(m); kb_.ay32.alloc(m); kb_.az32.alloc(m);
+    kb_.pcart.alloc(m); kb_.pbound.alloc(m);
+    int* rstart_b = take<int>(ctx, (long) kNL * kNL * nrow);
+    int* rlen_b = take<int>(ctx, (long) kNL * kNL * nrow);
+    LSJK_CUDA(cudaMemsetAsync(rstart_b, 0, sizeof(int) * kNL * kNL * nrow, s));
+    LSJK_CUDA(cudaMemsetAsync(rlen_b, 0, sizeof(int) * kNL * kNL * nrow, s));
+    k_kinv_fill<<<nblk(m, 256), 256, 0, s>>>(ent, perm_b, m, bidx->view(), bpart->view(), nullptr, kb_.kab.p,
+                                            kb_.p.p, kb_.ip.p, kb_.px.p, kb_.py.p, kb_.pz.p, kb_.ax.p, kb_.ay.p,
+                                            kb_.az.p, kb_.kab32.p, kb_.p32.p, kb_.ip32.p, kb_.px32.p, kb_.py32.p,
+                                            kb_.pz32.p, kb_.ax32.p, kb_.ay32.p, kb_.az32.p, kb_.pcart.p,
+                                            kb_.pbound.p, rstart_b, rlen_b, nrow);
+    LSJK_CUDA(cudaGetLastError());
     for (int a = 0; a < kNL; ++a)
         for (int b = 0; b < kNL; ++b) {
             long off = (long) (a * kNL + b) * nrow;
@@ -414,7 +448,7 @@ void build_kinv(Context* ctx, PairList* pl)
         }
     LSJK_CUDA(cudaStreamSynchronize(s));
     pl->kinv_built = true;
-    ctx->stats.kernel_launches += 16;
+    ctx->stats.kernel_launches += 20;
 }
 
 } // namespace lsjk
