@@ -400,7 +400,16 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             A.boys32 = ctx->boys32.p + (long) (LB + LK) * LSJK_BOYS_NBIN * 8;
             A.mixed = mixed ? 1 : 0;
             A.thredp = thredp;
-            A.chunk = ctx->tune.j_chunk[LB][LK] > 0 ? ctx->tune.j_chunk[LB][LK] : kJChunk;
+            if (ctx->tune.j_chunk[LB][LK] > 0) {
+                A.chunk = ctx->tune.j_chunk[LB][LK];
+            } else {
+                // default: kJChunk kets per CTA, halved (down to 64) while the grid would not
+                // give every multiprocessor two CTAs -- small molecules need the parallelism
+                const long tiles = (jb.n + kJThreads - 1) / kJThreads;
+                int chunk = kJChunk;
+                while (chunk > 64 && tiles * ((jk.n + chunk - 1) / chunk) < 2L * ctx->nsm) chunk >>= 1;
+                A.chunk = chunk;
+            }
             A.ng = ng;
             A.jbra_stride = (long) jb.n * nherm_of(LB);
             A.nterm = (int) ew.alpha.size();

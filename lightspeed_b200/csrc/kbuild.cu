@@ -72,6 +72,11 @@ struct TaskGenArgs {
     KTask* tasks;                  // per-combo regions
     long cap_off[kNCombo];         // region offsets (by value: graph-capturable)
     int* ntask;                    // per-combo counts
+    // mixed precision: tasks whose first quartet reaches thredp, the only ones the FP64 pass can use
+    KTask* tasks_hi;
+    int* ntask_hi;
+    float thredp;
+    int split;
 };
 
 __global__ void k_task_gen(TaskGenArgs A)
@@ -107,6 +112,10 @@ __global__ void k_task_gen(TaskGenArgs A)
             int c = combo_index(L1, L2, L3, L4);
             int slot = atomicAdd(&A.ntask[c], 1);
             A.tasks[A.cap_off[c] + slot] = KTask{i2, i4, dmax};
+            if (A.split && (double) (b12 * b34) * dmax >= (double) A.thredp) {
+                int hs = atomicAdd(&A.ntask_hi[c], 1);
+                A.tasks_hi[A.cap_off[c] + hs] = KTask{i2, i4, dmax};
+            }
         }
     }
 }
@@ -197,13 +206,14 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     off[c + 1] = (long) cnt2[L2] * cnt4[L4];
                 }
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
+    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
-    int* ntask = take<int>(ctx, kNCombo);
+    int* ntask = take<int>(ctx, 2 * kNCombo);   // all tasks, then the FP64-pass tasks
+    KTask* tasks_hi = mixed ? take<KTask>(ctx, off[kNCombo]) : nullptr;
     unsigned* queue = take<unsigned>(ctx, 2 * kNCombo * kKBatch);   // per class, pass and launch
     unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
     unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
-    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
-    LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
+    LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * 2 * kNCombo, s));
     LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo * kKBatch, s));
 
     TaskGenArgs G{};
@@ -227,6 +237,10 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     G.tasks = tasks;
     for (int c = 0; c < kNCombo; ++c) G.cap_off[c] = off[c];
     G.ntask = ntask;
+    G.tasks_hi = tasks_hi;
+    G.ntask_hi = ntask + kNCombo;
+    G.thredp = thredp;
+    G.split = mixed ? 1 : 0;
     if (b2->nprim && b4->nprim && pl12->kdat.nent && pl34->kdat.nent) {
         dim3 grid(nblk(b4->nprim, 128), b2->nprim);
         k_task_gen<<<grid, 128, 0, s>>>(G);
@@ -288,6 +302,11 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     const float inf = __builtin_huge_valf();
                     // FP64 pass: estimate >= thredp (mixed) or >= thresp (FP64 mode)
                     A.queue = queue + (long) c * kKBatch;
+                    if (mixed) {
+                        // FP64 pass: only the tasks that can reach thredp
+                        A.tasks = tasks_hi + off[c];
+                        A.ntask = ntask + kNCombo + c;
+                    }
                     A.thr_lo = mixed ? thredp : thresp;
                     A.thr_hi = inf;
                     A.rys = ctx->rys64.p + kRysOffset[NR];
@@ -327,7 +346,9 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     if (ctx->tuning) tune(A, false);
                     launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
                     if (mixed) {
-                        // FP32 pass: thresp <= estimate < thredp
+                        // FP32 pass: thresp <= estimate < thredp, over all tasks
+                        A.tasks = tasks + off[c];
+                        A.ntask = ntask + c;
                         A.queue = queue + (long) (kNCombo + c) * kKBatch;
                         A.thr_lo = thresp;
                         A.thr_hi = thredp;

@@ -20,6 +20,7 @@
 // into an FP64 pass and an FP32 pass in mixed mode.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 #include "kargs.cuh"
 #include "lsjk_device.cuh"
@@ -318,11 +319,13 @@ void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     const size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(R);
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    static std::atomic<unsigned long long> attr_devices{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_devices.load(std::memory_order_acquire) & bit)) {
         LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, R, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int) smem));
-        attr = true;
+        attr_devices.fetch_or(bit, std::memory_order_acq_rel);
     }
     k_exchange<L1, L2, L3, L4, R, NG><<<grid, kKThreads, smem, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
