@@ -576,8 +576,11 @@ def run_many(args):
     either (a) as a sequential per-molecule loop of device calls, or (b) as
     one CUDA graph holding every molecule's builds (captured once per active
     set, replayed while the set is unchanged), then J and K come back in one
-    copy. Reported per mode: molecules/s over the whole run, quartets/s over
-    the J/K phases (device events), and the wall time split."""
+    copy; (c) the same builds spread round-robin over 8 extra engine contexts
+    (ls.Stream: own CUDA stream and scratch) so small molecules' kernels run
+    concurrently. Reported per mode: molecules/s over the whole run,
+    quartets/s over the J/K phases (device events), and the wall time split.
+    `value` is the best mode's molecules/s."""
     rank, world, local = dist_info()
     import torch
     torch.cuda.set_device(local)
@@ -615,9 +618,21 @@ def run_many(args):
             ls.coulomb_device(ew, pl, pl, [ptr(D_dev, m)], [ptr(JK_dev[0], m)], thre, thre)
             ls.exchange_device(ew, pl, pl, [ptr(D_dev, m)], True, [ptr(JK_dev[1], m)], thre, thre)
 
+    # concurrent mode: molecules spread round-robin over extra engine contexts (own streams)
+    nstream = 8
+    extra = [ls.Stream() for _ in range(nstream)]
+    xstreams = [torch.cuda.ExternalStream(x.stream_handle(), device=dev) for x in extra]
+
+    def builds_concurrent(active):
+        for k, m in enumerate(active):
+            x = extra[k % nstream]
+            pl = systems[m][2].pairs
+            x.coulomb_device(ew, pl, pl, [ptr(D_dev, m)], [ptr(JK_dev[0], m)], thre, thre)
+            x.exchange_device(ew, pl, pl, [ptr(D_dev, m)], True, [ptr(JK_dev[1], m)], thre, thre)
+
     results = {}
     energies = {}
-    for mode in ("sequential", "graph"):
+    for mode in ("sequential", "graph", "streams"):
         steppers = [SCFStepper(r, sad.density(mol, bas), g_conv=1.0e-8) for mol, bas, r in systems]
         active = list(range(len(systems)))
         graph, graph_set = None, None
@@ -635,7 +650,14 @@ def run_many(args):
                 JK_dev.zero_()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                if mode == "graph" and graph is not None and graph_set == active:
+                if mode == "streams":
+                    for xs in xstreams:          # the extra streams start after the copies
+                        xs.wait_event(e0)
+                    builds_concurrent(active)
+                    for xs in xstreams:
+                        stream.wait_stream(xs)
+                    e1.record(stream)
+                elif mode == "graph" and graph is not None and graph_set == active:
                     graph.launch()
                     e1.record(stream)
                 else:
@@ -664,6 +686,9 @@ def run_many(args):
         wall = time.time() - t_start
         stt = ls.stats()
         q = stt["j_quartets"] + stt["k_quartets"]
+        if mode == "streams":
+            # the extra contexts keep their own counters; the work equals the sequential mode's
+            q = results["sequential"]["quartets"]
         energies[mode] = np.array([r.E for _, _, r in systems])
         results[mode] = {"seconds": wall, "molecules_per_s": len(systems) / wall, "lockstep_iterations": iters,
                          "jk_gpu_seconds": gpu_ms * 1e-3, "quartets": q,
@@ -672,16 +697,18 @@ def run_many(args):
                          "gpu_launches": stt["kernel_launches"]}
         del graph
     line = {
-        "metric": "many-molecule batch: molecules/s and quartets/s, one CUDA graph per SCF iteration vs "
-                  "a sequential per-molecule GPU loop",
-        "value": results["graph"]["molecules_per_s"], "unit": "molecules/s", "n_gpus": 1,
+        "metric": "many-molecule batch: molecules/s and quartets/s; one CUDA graph per SCF iteration, or "
+                  "8 concurrent engine streams, vs a sequential per-molecule GPU loop",
+        "value": max(r["molecules_per_s"] for r in results.values()), "unit": "molecules/s", "n_gpus": 1,
         "higher_is_better": True, "data": "synthetic", "dtype": "f64",
         "config": {"workload": "%d water clusters of 1-12 H2O (sizes from seed 0, cluster m from seed m), 6-31G*, "
                                "RHF from SAD to 1e-8" % len(systems), "thresp": thre,
                    "total_functions": int(sum(naos)), "setup_seconds": t_setup},
-        "sequential": results["sequential"], "graph": results["graph"],
+        "sequential": results["sequential"], "graph": results["graph"], "streams": results["streams"],
         "speedup_graph_vs_sequential": results["sequential"]["seconds"] / results["graph"]["seconds"],
+        "speedup_streams_vs_sequential": results["sequential"]["seconds"] / results["streams"]["seconds"],
         "max_abs_dE_graph_vs_sequential": float(np.max(np.abs(energies["graph"] - energies["sequential"]))),
+        "max_abs_dE_streams_vs_sequential": float(np.max(np.abs(energies["streams"] - energies["sequential"]))),
     }
     print(json.dumps(line))
     return 0

@@ -248,6 +248,56 @@ PYBIND11_MODULE(_lightspeed, m)
         check_rc(lsjk_measure_fma_peak(Engine::instance().ctx(), fp64 ? 1 : 0, &t), "fma_peak");
         return t;
     }, py::arg("fp64") = true);
+    // An additional engine context with its own CUDA stream, scratch and
+    // counters, for running independent builds concurrently (e.g. the J/K of
+    // different molecules): pair lists and bases are shared with the main
+    // context; calls on one Stream are ordered, different Streams overlap.
+    struct ExtraContext {
+        lsjk_context* c = nullptr;
+        explicit ExtraContext(int device)
+        {
+            check_rc(lsjk_context_create(device, &c), "Stream");
+            check_rc(lsjk_context_set_precision(c, Engine::instance().precision()), "Stream");
+        }
+        ~ExtraContext() { if (c) lsjk_context_destroy(c); }
+    };
+    py::class_<ExtraContext, std::shared_ptr<ExtraContext>>(m, "Stream")
+        .def(py::init([]() { return std::make_shared<ExtraContext>(Engine::instance().device()); }))
+        .def("set_precision", [](ExtraContext& x, int mode) { check_rc(lsjk_context_set_precision(x.c, mode),
+                                                                       "Stream.set_precision"); })
+        .def("stream_handle", [](ExtraContext& x) { return (uintptr_t) lsjk_context_stream(x.c); })
+        .def("coulomb_device", [](ExtraContext& x, const std::shared_ptr<Ewald>& ew,
+                                  const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,
+                                  const std::vector<uintptr_t>& D, const std::vector<uintptr_t>& J, float thresp,
+                                  float thredp) {
+            if (D.size() != J.size()) throw std::runtime_error("coulomb_device: D/J count mismatch");
+            std::vector<const double*> dp;
+            std::vector<double*> jp;
+            for (size_t k = 0; k < D.size(); ++k) {
+                dp.push_back(reinterpret_cast<const double*>(D[k]));
+                jp.push_back(reinterpret_cast<double*>(J[k]));
+            }
+            check_rc(lsjk_coulomb_device(x.c, (int) ew->scales().size(), ew->scales().data(), ew->omegas().data(),
+                                         pl12->device_handle(), pl34->device_handle(), (int) dp.size(), dp.data(),
+                                         thresp, thredp, jp.data()),
+                     "Stream.coulomb_device");
+        }, py::call_guard<py::gil_scoped_release>())
+        .def("exchange_device", [](ExtraContext& x, const std::shared_ptr<Ewald>& ew,
+                                   const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,
+                                   const std::vector<uintptr_t>& D, bool D24symm, const std::vector<uintptr_t>& K,
+                                   float thresp, float thredp) {
+            if (D.size() != K.size()) throw std::runtime_error("exchange_device: D/K count mismatch");
+            std::vector<const double*> dp;
+            std::vector<double*> kp;
+            for (size_t k = 0; k < D.size(); ++k) {
+                dp.push_back(reinterpret_cast<const double*>(D[k]));
+                kp.push_back(reinterpret_cast<double*>(K[k]));
+            }
+            check_rc(lsjk_exchange_device(x.c, (int) ew->scales().size(), ew->scales().data(), ew->omegas().data(),
+                                          pl12->device_handle(), pl34->device_handle(), (int) dp.size(), dp.data(),
+                                          D24symm ? 1 : 0, thresp, thredp, kp.data()),
+                     "Stream.exchange_device");
+        }, py::call_guard<py::gil_scoped_release>());
     // Device-resident J/K: D and J/K are device addresses (e.g. torch
     // tensor.data_ptr()); the work is enqueued on the engine stream only.
     m.def("coulomb_device", [](const std::shared_ptr<Ewald>& ew, const std::shared_ptr<PairList>& pl12,

@@ -15,7 +15,9 @@ of a shell share one normalisation, so monomials transform like the basis
 functions). The inputs are rotation invariant: the pair type, 16 Gaussian
 radial shells of the distance, J's position in I's frame and I's in J's,
 the relative orientation F_I F_J^T, and per atom 16-shell radial symmetry
-functions (Behler type, cutoff 6 Angstrom) for H and O neighbours.
+functions (Behler type, cutoff 6 Angstrom) for H and O neighbours plus the
+positions, in the atom's frame, of its three nearest O and three nearest H
+atoms of other waters.
 
 The network's weights, activations and gradients are bfloat16 and every
 product accumulates in FP32 (kernels: lsmlp_* in liblsjk.so); master weights
@@ -36,7 +38,9 @@ R_CUT = 6.0                     # Angstrom
 MU = np.linspace(0.5, R_CUT, N_RADIAL)
 ETA = 1.0 / (2.0 * (MU[1] - MU[0]) ** 2)
 PAIR_TYPES = ("O*", "H*", "OO", "OH", "HH")   # self blocks, then I < J pairs (O before H)
-N_FEAT = len(PAIR_TYPES) + N_RADIAL + 3 + 3 + 9 + 2 * 2 * N_RADIAL
+N_NEIGH = 3                     # nearest O and nearest H of other waters, per atom
+N_ENV = 2 * N_NEIGH * 3         # their positions in the atom's frame
+N_FEAT = len(PAIR_TYPES) + N_RADIAL + 3 + 3 + 9 + 2 * (2 * N_RADIAL + N_ENV)
 WIDTH = 256
 N_OUT = 15 * 15
 
@@ -145,16 +149,41 @@ def pair_list(xyz_ang, symbols):
     return pairs
 
 
-def pair_features(xyz_bohr, symbols, pairs, F, G):
+def atom_environments(xyz_ang, symbols, F):
+    """(natom, N_ENV): for each atom, the N_NEIGH nearest O and H atoms of other
+    waters, as positions in the atom's frame scaled by the cutoff function
+    (zero padded), nearest first."""
+    n = len(symbols)
+    isO = np.array([s.upper() == "O" for s in symbols])
+    water = np.arange(n) // 3
+    E = np.zeros((n, N_ENV))
+    for i in range(n):
+        v = xyz_ang - xyz_ang[i]
+        d = np.linalg.norm(v, axis=1)
+        other = (water != water[i]) & (d < R_CUT)
+        for s_idx, sel in enumerate((isO, ~isO)):
+            cand = np.nonzero(other & sel)[0]
+            cand = cand[np.argsort(d[cand])][:N_NEIGH]
+            for k, j in enumerate(cand):
+                off = (s_idx * N_NEIGH + k) * 3
+                E[i, off:off + 3] = (F[i] @ v[j]) * _cutoff(d[j])
+    return E
+
+
+def pair_features(xyz_bohr, symbols, pairs, F, G, Env):
     xyz = xyz_bohr * ANG_PER_BOHR
-    X = np.zeros((len(pairs), N_FEAT), np.float32)
-    for k, (i, j, t) in enumerate(pairs):
-        v = xyz[j] - xyz[i]
-        r = np.linalg.norm(v)
-        f = [np.eye(len(PAIR_TYPES))[t], np.exp(-ETA * (r - MU) ** 2), F[i] @ v, F[j] @ (-v),
-             (F[i] @ F[j].T).ravel(), G[i], G[j]]
-        X[k] = np.concatenate(f)
-    return X
+    P = np.array(pairs, dtype=np.int64).reshape(-1, 3)
+    I, J, T = P[:, 0], P[:, 1], P[:, 2]
+    v = xyz[J] - xyz[I]
+    r = np.linalg.norm(v, axis=1)
+    X = np.concatenate([
+        np.eye(len(PAIR_TYPES))[T],
+        np.exp(-ETA * (r[:, None] - MU[None, :]) ** 2),
+        np.einsum("pab,pb->pa", F[I], v),
+        np.einsum("pab,pb->pa", F[J], -v),
+        np.einsum("pab,pcb->pac", F[I], F[J]).reshape(-1, 9),
+        G[I], Env[I], G[J], Env[J]], axis=1)
+    return X.astype(np.float32)
 
 
 def local_targets(D, pairs, maps):
@@ -382,8 +411,9 @@ def water_pairs_data(mol, basis):
     xyz = np.array(mol.xyz)
     F = water_frames(xyz, symbols)
     G = atom_descriptors(xyz * ANG_PER_BOHR, symbols)
+    Env = atom_environments(xyz * ANG_PER_BOHR, symbols, F)
     pairs = pair_list(xyz * ANG_PER_BOHR, symbols)
-    X = pair_features(xyz, symbols, pairs, F, G)
+    X = pair_features(xyz, symbols, pairs, F, G, Env)
     maps = atom_maps(basis, F)
     return pairs, X, maps
 

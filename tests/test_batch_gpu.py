@@ -79,3 +79,42 @@ def test_multi_fp64_vs_oracle(ls):
             assert np.max(abs(J.np - Jr)) < 1e-10
     finally:
         ls.set_precision(ls.PREC_MIXED)
+
+
+def test_concurrent_streams_match_engine(ls):
+    """Builds enqueued on two extra engine contexts (ls.Stream, own CUDA
+    streams and scratch) for two different molecules at once equal the main
+    context's builds (1e-10): the contexts share pair lists but nothing else."""
+    import torch
+    from lightspeed_b200.geometry import water_cluster
+    ls.set_precision(ls.PREC_FP64)
+    try:
+        res = ls.ResourceList.build()
+        ew = ls.Ewald.coulomb()
+        mols = []
+        for n, seed in ((3, 21), (4, 22)):
+            bas = ls.Basis.from_gbs_file(water_cluster(n, seed=seed), "6-31gs")
+            pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+            D = _densities(1, bas.nao, seed)[0]
+            D = D + D.T
+            J1 = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), 1e-14, 1e-14).np
+            K1 = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-14).np
+            mols.append((pl, D, J1, K1))
+        streams = [ls.Stream(), ls.Stream()]
+        out = []
+        for (pl, D, _, _), st in zip(mols, streams):
+            Dd = torch.tensor(D, device="cuda")
+            Jd = torch.zeros_like(Dd)
+            Kd = torch.zeros_like(Dd)
+            out.append((Dd, Jd, Kd))
+        torch.cuda.synchronize()
+        for (pl, _, _, _), st, (Dd, Jd, Kd) in zip(mols, streams, out):
+            st.coulomb_device(ew, pl, pl, [Dd.data_ptr()], [Jd.data_ptr()], 1e-14, 1e-14)
+            st.exchange_device(ew, pl, pl, [Dd.data_ptr()], True, [Kd.data_ptr()], 1e-14, 1e-14)
+        for st in streams:
+            torch.cuda.ExternalStream(st.stream_handle()).synchronize()
+        for (_, _, J1, K1), (_, Jd, Kd) in zip(mols, out):
+            assert np.max(np.abs(Jd.cpu().numpy() - J1)) < 1e-10
+            assert np.max(np.abs(Kd.cpu().numpy() - K1)) < 1e-10
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
