@@ -249,6 +249,11 @@ int lsjk_context_create(int device, lsjk_context** out)
             LSJK_CUDA(cudaEventCreate(&c.ev0));
             LSJK_CUDA(cudaEventCreate(&c.ev1));
             LSJK_CUDA(cudaEventCreate(&c.ev2));
+            for (int i = 0; i < lsjk::Context::kAux; ++i) {
+                LSJK_CUDA(cudaStreamCreateWithFlags(&c.aux[i], cudaStreamNonBlocking));
+                LSJK_CUDA(cudaEventCreateWithFlags(&c.join_ev[i], cudaEventDisableTiming));
+            }
+            LSJK_CUDA(cudaEventCreateWithFlags(&c.fork_ev, cudaEventDisableTiming));
             LSJK_CUDA(cudaStreamSynchronize(c.stream));
         } catch (...) {
             delete h;
@@ -267,6 +272,14 @@ int lsjk_context_destroy(lsjk_context* ctx)
         if (ctx->c.ev0) cudaEventDestroy(ctx->c.ev0);
         if (ctx->c.ev1) cudaEventDestroy(ctx->c.ev1);
         if (ctx->c.ev2) cudaEventDestroy(ctx->c.ev2);
+        for (int i = 0; i < lsjk::Context::kAux; ++i) {
+            if (ctx->c.aux[i]) {
+                cudaStreamSynchronize(ctx->c.aux[i]);
+                cudaStreamDestroy(ctx->c.aux[i]);
+            }
+            if (ctx->c.join_ev[i]) cudaEventDestroy(ctx->c.join_ev[i]);
+        }
+        if (ctx->c.fork_ev) cudaEventDestroy(ctx->c.fork_ev);
         cudaStream_t s = ctx->c.stream;
         delete ctx;
         if (s) cudaStreamDestroy(s);

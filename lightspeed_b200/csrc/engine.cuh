@@ -182,6 +182,13 @@ struct Context {
     DBuf<unsigned long long> counters;  // quartet counters and work queues
     lsjk_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+    // auxiliary streams: the per-class J and K kernels of one build are spread
+    // over them (fork after the shared set-up, join before the back
+    // transforms), so one class's tail overlaps the next class's start
+    static constexpr int kAux = 4;
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[kAux] = {};
     // scratch buffers reused across calls (grown on demand)
     std::vector<std::unique_ptr<DBuf<char>>> scratch;
     size_t scratch_used = 0;
@@ -217,6 +224,31 @@ inline char* Context::scratch_take(size_t bytes)
     scratch_used = used + bytes;
     return scratch.back()->p;
 }
+
+// Make the auxiliary streams wait for the work enqueued so far on ctx->stream.
+inline void fork_aux(Context* ctx)
+{
+    LSJK_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    for (int i = 0; i < Context::kAux; ++i) LSJK_CUDA(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
+}
+
+// Make ctx->stream wait for everything enqueued on the auxiliary streams.
+inline void join_aux(Context* ctx)
+{
+    for (int i = 0; i < Context::kAux; ++i) {
+        LSJK_CUDA(cudaEventRecord(ctx->join_ev[i], ctx->aux[i]));
+        LSJK_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join_ev[i], 0));
+    }
+}
+
+// While alive, ctx->stream is auxiliary stream i (the launchers enqueue on
+// ctx->stream); restores the main stream on exit.
+struct OnAux {
+    Context* ctx;
+    cudaStream_t main;
+    OnAux(Context* c, int i) : ctx(c), main(c->stream) { c->stream = c->aux[i % Context::kAux]; }
+    ~OnAux() { ctx->stream = main; }
+};
 
 template <typename T>
 inline T* take(Context* ctx, size_t n) { return reinterpret_cast<T*>(ctx->scratch_take(sizeof(T) * (n ? n : 1))); }

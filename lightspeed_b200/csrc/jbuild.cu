@@ -17,6 +17,7 @@
 //     symmetric-list double write and 1/2 on diagonal primitive pairs.
 #include <algorithm>
 #include <cub/device/device_radix_sort.cuh>
+#include <optional>
 #include "engine.cuh"
 #include "hermite.cuh"
 #include "jargs.cuh"
@@ -378,6 +379,11 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
         jbra[LB] = take<double>(ctx, (long) DS.slots * n * nherm_of(LB));
         LSJK_CUDA(cudaMemsetAsync(jbra[LB], 0, sizeof(double) * DS.slots * n * nherm_of(LB), s));
     }
+    // class kernels go round-robin to the auxiliary streams (not while the
+    // autotuner times them one by one)
+    const bool par = !ctx->tuning;
+    if (par) fork_aux(ctx);
+    int lane = 0;
     for (int LB = 0; LB < kNHerm; ++LB) {
         const JBraClass& jb = pl12->jb[LB];
         if (!jb.n) continue;
@@ -453,9 +459,12 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
                 }
                 A.chunk = ctx->tune.j_chunk[LB][LK];
             }
+            std::optional<OnAux> on;
+            if (par) on.emplace(ctx, lane++);
             launch(A);
         }
     }
+    if (par) join_aux(ctx);
 
     // 5. back to Cartesian, per density
     for (int g = 0; g < ng; ++g)

@@ -18,6 +18,7 @@
 //     contracts with D24 in registers, then scatters the K13 block with FP64
 //     atomics. No ERI is stored.
 #include <algorithm>
+#include <optional>
 #include "engine.cuh"
 #include "lsjk_device.cuh"
 #include "kargs.cuh"
@@ -250,6 +251,11 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
         return;
     }
 
+    // class kernels go round-robin to the auxiliary streams (not while the
+    // autotuner times them one by one)
+    const bool par = !ctx->tuning;
+    if (par) fork_aux(ctx);
+    int lane = 0;
     for (int L1 = 0; L1 < kNL; ++L1)
         for (int L2 = 0; L2 < kNL; ++L2)
             for (int L3 = 0; L3 < kNL; ++L3)
@@ -344,7 +350,11 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned) * kKBatch, s));
                     };
                     if (ctx->tuning) tune(A, false);
-                    launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
+                    {
+                        std::optional<OnAux> on;
+                        if (par) on.emplace(ctx, lane++);
+                        launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
+                    }
                     if (mixed) {
                         // FP32 pass: thresp <= estimate < thredp, over all tasks
                         A.tasks = tasks + off[c];
@@ -357,9 +367,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         A.asym_w = ctx->rys_asym32.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
                         A.qcount = qcnt32 + c;
                         if (ctx->tuning) tune(A, true);
+                        std::optional<OnAux> on;
+                        if (par) on.emplace(ctx, lane++);
                         launch_k1(ctx, A, cap, L1, L2, L3, L4, true);
                     }
                 }
+    if (par) join_aux(ctx);
 }
 
 } // namespace lsjk
