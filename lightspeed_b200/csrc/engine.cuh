@@ -185,7 +185,7 @@ struct Context {
     // auxiliary streams: the per-class J and K kernels of one build are spread
     // over them (fork after the shared set-up, join before the back
     // transforms), so one class's tail overlaps the next class's start
-    static constexpr int kAux = 4;
+    static constexpr int kAux = 8;
     cudaStream_t aux[kAux] = {};
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t join_ev[kAux] = {};
