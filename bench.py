@@ -639,6 +639,8 @@ def run_many(args):
         t_start = time.time()
         gpu_ms, iters, q = 0.0, 0, 0
         ls.reset_stats()
+        for x in extra:
+            x.reset_stats()
         Dh = D_host.numpy()
         JKh = JK_host.numpy()
         while active and iters < 100:
@@ -684,11 +686,11 @@ def run_many(args):
         for st in steppers:
             st.finish()
         wall = time.time() - t_start
-        stt = ls.stats()
+        stt = dict(ls.stats())
+        for x in extra:                    # the extra contexts keep their own counters
+            for key, val in x.stats().items():
+                stt[key] += val
         q = stt["j_quartets"] + stt["k_quartets"]
-        if mode == "streams":
-            # the extra contexts keep their own counters; the work equals the sequential mode's
-            q = results["sequential"]["quartets"]
         energies[mode] = np.array([r.E for _, _, r in systems])
         results[mode] = {"seconds": wall, "molecules_per_s": len(systems) / wall, "lockstep_iterations": iters,
                          "jk_gpu_seconds": gpu_ms * 1e-3, "quartets": q,

@@ -36,10 +36,10 @@ std::shared_ptr<Tensor> tensor_from_array(py::array_t<double, py::array::c_style
     return t;
 }
 
-py::dict stats_dict()
+py::dict stats_dict_of(lsjk_context* ctx)
 {
     lsjk_stats st{};
-    check_rc(lsjk_context_stats(Engine::instance().ctx(), &st), "stats");
+    check_rc(lsjk_context_stats(ctx, &st), "stats");
     py::dict d;
     d["quartets_fp64"] = st.quartets_fp64;
     d["quartets_fp32"] = st.quartets_fp32;
@@ -50,6 +50,8 @@ py::dict stats_dict()
     d["kernel_launches"] = st.kernel_launches;
     return d;
 }
+
+py::dict stats_dict() { return stats_dict_of(Engine::instance().ctx()); }
 
 } // namespace
 
@@ -266,6 +268,8 @@ PYBIND11_MODULE(_lightspeed, m)
         .def("set_precision", [](ExtraContext& x, int mode) { check_rc(lsjk_context_set_precision(x.c, mode),
                                                                        "Stream.set_precision"); })
         .def("stream_handle", [](ExtraContext& x) { return (uintptr_t) lsjk_context_stream(x.c); })
+        .def("stats", [](ExtraContext& x) { return stats_dict_of(x.c); })
+        .def("reset_stats", [](ExtraContext& x) { check_rc(lsjk_context_reset_stats(x.c), "Stream.reset_stats"); })
         .def("coulomb_device", [](ExtraContext& x, const std::shared_ptr<Ewald>& ew,
                                   const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,
                                   const std::vector<uintptr_t>& D, const std::vector<uintptr_t>& J, float thresp,

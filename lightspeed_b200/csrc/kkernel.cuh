@@ -132,8 +132,7 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
         }
         R t2[NR], w[NR];
         rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
+        auto root = [&](int r) {
             const R u = t2[r] * d2 * ipq;
             const R qu = q * u, pu = p * u;
             const R c00x = PAx - qu * PQx, c00y = PAy - qu * PQy, c00z = PAz - qu * PQz;
@@ -143,6 +142,14 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
             for (int g = 0; g < NG; ++g)
                 kq_dispatch<L1, L2, L3, L4>(c00x, c00y, c00z, d00x, d00y, d00z, b00, b10, b01, e.ax, e.ay, e.az,
                                             Cx, Cy, Cz, f * w[r], Dblk[g], KV[g]);
+        };
+        if constexpr (sizeof(R) == 4) {
+            // FP32: roots one after another (fewer live registers, more resident warps)
+#pragma unroll 1
+            for (int r = 0; r < NR; ++r) root(r);
+        } else {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) root(r);
         }
     }
 #pragma unroll
