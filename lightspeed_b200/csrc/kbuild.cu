@@ -37,6 +37,24 @@ constexpr int kNCombo = kNL * kNL * kNL * kNL;
 
 
 
+// K = K + K^T in place (square ld x ld): the transposed half of the symmetric
+// D24 contributions, which the class kernels do not write.
+__global__ void k_symmetrize(double* __restrict__ K, int n)
+{
+    const long total = (long) n * n;
+    for (long k = blockIdx.x * (long) blockDim.x + threadIdx.x; k < total; k += (long) gridDim.x * blockDim.x) {
+        const int i = (int) (k / n), j = (int) (k % n);
+        if (i > j) continue;
+        if (i == j) {
+            K[k] *= 2.0;
+        } else {
+            const double v = K[k] + K[(long) j * n + i];
+            K[k] = v;
+            K[(long) j * n + i] = v;
+        }
+    }
+}
+
 __global__ void k_absmax(const double* __restrict__ X, long n, unsigned long long* __restrict__ out)
 {
     double m = 0.0;
@@ -373,6 +391,15 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     }
                 }
     if (par) join_aux(ctx);
+    if (flip_ok) {
+        // basis 1 == basis 3 here, so each K13 is square
+        const int n = b3->ncart;
+        for (int g = 0; g < ng; ++g) {
+            k_symmetrize<<<std::min<long>(nblk((long) n * n, 256), 1184), 256, 0, s>>>(Kcart[g], n);
+            LSJK_CUDA(cudaGetLastError());
+            ctx->stats.kernel_launches++;
+        }
+    }
 }
 
 } // namespace lsjk

@@ -10,7 +10,9 @@
 // cp.async (the next 32 are in flight while the current 32 are used) and read
 // as broadcasts. Partners 1 come grouped by contracted shell, so a lane sums
 // the quartets of one shell segment -- same K13 target block -- in registers
-// and issues one FP64 atomic per element when the segment ends.
+// and issues one FP64 atomic per element when the segment ends (for a
+// symmetric D24 only the untransposed one: the build symmetrises K13 after
+// the class kernels).
 // Up to k_batch densities share a launch: the integrals of a quartet are
 // formed once and contracted with each density's D24 block.
 // Screens (per quartet, exactly the reference's set):
@@ -193,7 +195,10 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
         const KTask T = A.tasks[task];
         const int i2 = T.i2, i4 = T.i4;
         const double dmax = T.dmax;   // largest |D24 block| over the densities of the batch
-        const bool flip = A.flip && i2 != i4;
+        // symmetric D24 (A.flip): the transposed contribution of a task with i2 != i4 is not
+        // written here; the build adds K13 to its transpose afterwards, and tasks with
+        // i2 == i4 (whose contribution is symmetric) enter with weight 1/2
+        const double wsym = (A.flip && i2 == i4) ? 0.5 : 1.0;
         // per-task float thresholds on the bound product (exactly the double screens)
         const float tlo = float_threshold(thr_lo, dmax);
         const float thi = float_threshold(thr_hi, dmax);
@@ -260,8 +265,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                         for (int a = 0; a < N1; ++a)
 #pragma unroll
                             for (int c = 0; c < N3; ++c) {
-                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], acc[g][a * N3 + c]);
-                                if (flip) atomicAdd(&Kc[(long) (c3 + c) * A.ld3 + prev_c1 + a], acc[g][a * N3 + c]);
+                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * acc[g][a * N3 + c]);
                                 acc[g][a * N3 + c] = 0.0;
                             }
                     }
