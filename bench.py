@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--train-clusters", type=int, default=1000)
     ap.add_argument("--test-clusters", type=int, default=20)
     ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--guess-norm", default="element", choices=["element", "type"])
     ap.add_argument("--profile-step", action="store_true",
                     help="after set-up and warm-up, run one FP64 J+K step between cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off) and exit")
@@ -539,7 +540,7 @@ def run_guess(args):
     t_data = time.time() - t0
     net = g.MLP(ls, seed=0)
     t0 = time.time()
-    hist = net.fit(X, Y, W, epochs=args.epochs, batch=4096, lr=2e-3)
+    hist = net.fit(X, Y, W, epochs=args.epochs, batch=4096, lr=2e-3, norm=args.guess_norm)
     torch.cuda.synchronize()
     t_train = time.time() - t0
     # warm the SCF path once so neither arm pays first-call costs
@@ -553,7 +554,8 @@ def run_guess(args):
         "higher_is_better": True, "data": "synthetic", "dtype": "bf16 network, f64 SCF",
         "config": {"workload": "learned SCF guess", "train_clusters": len(train), "train_sizes": "4-16 H2O",
                    "test_clusters": len(test), "test_sizes": "20-24 H2O", "noise": "+-0.05 A, +-5 deg",
-                   "train_pairs": int(X.shape[0]), "epochs": args.epochs, "network": "3 x 256 SiLU, bf16"},
+                   "train_pairs": int(X.shape[0]), "epochs": args.epochs, "network": "3 x 256 SiLU, bf16",
+                   "target_scaling": args.guess_norm},
         "seconds_training_data": t_data, "seconds_training": t_train,
         "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
         "sad": {"iterations_mean": float(np.mean([r["sad"]["iterations"] for r in rows])), "seconds": t_sad},
@@ -578,7 +580,9 @@ def run_many(args):
     set, replayed while the set is unchanged), then J and K come back in one
     copy; (c) the same builds spread round-robin over 8 extra engine contexts
     (ls.Stream: own CUDA stream and scratch) so small molecules' kernels run
-    concurrently. Reported per mode: molecules/s over the whole run,
+    concurrently; (d) as (c) with the SCF algebra itself batched on the GPU
+    (scf_batched.BatchedRHF: molecules grouped by size, FP64 batched DIIS and
+    eigensolver), so the densities never leave the device. Reported per mode: molecules/s over the whole run,
     quartets/s over the J/K phases (device events), and the wall time split.
     `value` is the best mode's molecules/s."""
     rank, world, local = dist_info()
@@ -632,6 +636,46 @@ def run_many(args):
 
     results = {}
     energies = {}
+    # (d) everything on the GPU: batched SCF algebra (scf_batched) on device tensors that the
+    # concurrent contexts' builds read and write in place -- no per-iteration host copies
+    from lightspeed_b200.scf_batched import BatchedRHF
+    t_start = time.time()
+    for x in extra:
+        x.reset_stats()
+    ls.reset_stats()
+    bat = BatchedRHF(ls, [r for _, _, r in systems], dev)
+    bat.set_guess([sad.density(mol, bas) for mol, bas, _ in systems])
+    gpu_ms = 0.0
+    cur = torch.cuda.current_stream(dev)
+    while not bat.finished() and bat.iteration < 100:
+        bat.prepare()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        for xs in xstreams:
+            xs.wait_event(e0)
+        for k, (gi, b) in enumerate(bat.active()):
+            dptr, jptr, kptr = bat.targets(gi, b)
+            pl = systems[bat.groups[gi]["idx"][b]][2].pairs
+            x = extra[k % nstream]
+            x.coulomb_device(ew, pl, pl, [dptr], [jptr], thre, thre)
+            x.exchange_device(ew, pl, pl, [dptr], True, [kptr], thre, thre)
+        for xs in xstreams:
+            cur.wait_stream(xs)
+        e1.record(cur)
+        bat.update(1.0e-8)
+        e1.synchronize()
+        gpu_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    wall = time.time() - t_start
+    stt = dict(ls.stats())
+    for x in extra:
+        for key, val in x.stats().items():
+            stt[key] += val
+    q = stt["j_quartets"] + stt["k_quartets"]
+    energies["device"] = bat.energies()
+    results["device"] = {"seconds": wall, "molecules_per_s": len(systems) / wall, "lockstep_iterations": bat.iteration,
+                         "jk_gpu_seconds": gpu_ms * 1e-3, "quartets": q, "quartets_per_s": q / max(gpu_ms * 1e-3, 1e-12),
+                         "converged": int(bat.converged().sum()), "gpu_launches": stt["kernel_launches"]}
     for mode in ("sequential", "graph", "streams"):
         steppers = [SCFStepper(r, sad.density(mol, bas), g_conv=1.0e-8) for mol, bas, r in systems]
         active = list(range(len(systems)))
@@ -699,14 +743,17 @@ def run_many(args):
                          "gpu_launches": stt["kernel_launches"]}
         del graph
     line = {
-        "metric": "many-molecule batch: molecules/s and quartets/s; one CUDA graph per SCF iteration, or "
-                  "8 concurrent engine streams, vs a sequential per-molecule GPU loop",
+        "metric": "many-molecule batch: molecules/s and quartets/s; one CUDA graph per SCF iteration, 8 "
+                  "concurrent engine streams, or a GPU-resident batched SCF, vs a sequential per-molecule loop",
         "value": max(r["molecules_per_s"] for r in results.values()), "unit": "molecules/s", "n_gpus": 1,
         "higher_is_better": True, "data": "synthetic", "dtype": "f64",
         "config": {"workload": "%d water clusters of 1-12 H2O (sizes from seed 0, cluster m from seed m), 6-31G*, "
                                "RHF from SAD to 1e-8" % len(systems), "thresp": thre,
                    "total_functions": int(sum(naos)), "setup_seconds": t_setup},
         "sequential": results["sequential"], "graph": results["graph"], "streams": results["streams"],
+        "device": results["device"],
+        "speedup_device_vs_sequential": results["sequential"]["seconds"] / results["device"]["seconds"],
+        "max_abs_dE_device_vs_sequential": float(np.max(np.abs(energies["device"] - energies["sequential"]))),
         "speedup_graph_vs_sequential": results["sequential"]["seconds"] / results["graph"]["seconds"],
         "speedup_streams_vs_sequential": results["sequential"]["seconds"] / results["streams"]["seconds"],
         "max_abs_dE_graph_vs_sequential": float(np.max(np.abs(energies["graph"] - energies["sequential"]))),

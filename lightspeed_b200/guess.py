@@ -356,7 +356,11 @@ class MLP:
             k("lsmlp_adam", _p(w), _p(g), _p(m), _p(v), _p(wb), w.numel(), lr, 0.9, 0.999, 1e-8, self.step,
               wd if idx < len(self.W) else 0.0, s)
 
-    def fit(self, X, Y, Wm, epochs=40, batch=2048, lr=2e-3, seed=0, log=None):
+    def fit(self, X, Y, Wm, epochs=40, batch=2048, lr=2e-3, seed=0, log=None, norm="element"):
+        """Train on features X, targets Y with mask Wm. norm = "element": targets
+        standardised per pair type and block element; "type": centred per
+        element but scaled by one spread per pair type (the loss then weights
+        elements by their own spread, i.e. absolute error within a type)."""
         torch = self.torch
         X = torch.as_tensor(X, device=self.dev, dtype=torch.float32)
         self.x_mean = X.mean(0)
@@ -373,7 +377,11 @@ class MLP:
             mu = (Yt[sel] * w).sum(0) / cnt
             var = (((Yt[sel] - mu) ** 2) * w).sum(0) / cnt
             self.y_mean[t] = mu
-            self.y_std[t] = var.sqrt().clamp_min(1e-4)
+            if norm == "type":
+                tot = float((((Yt[sel] - mu) ** 2) * w).sum().item() / max(float(w.sum().item()), 1.0))
+                self.y_std[t] = max(tot, 1e-8) ** 0.5
+            else:
+                self.y_std[t] = var.sqrt().clamp_min(1e-4)
         Yt = (Yt - self.y_mean[ptype]) / self.y_std[ptype] * Wt
         Xb = self._prep(X)
         n = X.shape[0]
