@@ -330,14 +330,24 @@ void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     const size_t smem = (size_t) 2 * NR * A.nbin * 8 * sizeof(R);
-    // the shared-memory opt-in is a per-device function attribute: set it once per device
+    // the shared-memory opt-in is a per-device function attribute: set it once per
+    // device, and read how many CTAs of this kernel fit on a multiprocessor
     static std::atomic<unsigned long long> attr_devices{0};
-    const unsigned long long bit = 1ull << (ctx->device & 63);
+    static std::atomic<int> resident[64];
+    const int dev = ctx->device & 63;
+    const unsigned long long bit = 1ull << dev;
     if (!(attr_devices.load(std::memory_order_acquire) & bit)) {
         LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, R, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int) smem));
+        int occ = 0;
+        LSJK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exchange<L1, L2, L3, L4, R, NG>, kKThreads,
+                                                                smem));
+        resident[dev].store(occ > 0 ? occ : 1, std::memory_order_relaxed);
         attr_devices.fetch_or(bit, std::memory_order_acq_rel);
     }
+    // warps take tasks from the queue until it is empty, so CTAs beyond one
+    // resident wave would only start, find no work and leave
+    grid = std::min<unsigned>(grid, (unsigned) (ctx->nsm * resident[dev].load(std::memory_order_relaxed)));
     k_exchange<L1, L2, L3, L4, R, NG><<<grid, kKThreads, smem, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
