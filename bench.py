@@ -269,7 +269,8 @@ def run_ours(args):
         ls.reset_stats()
         step(THREDP)
         torch.cuda.synchronize()
-        counts[name] = ls.stats()
+        counts[name] = dict(ls.stats())
+        counts[name].update({"flops_" + k: v for k, v in ls.flops_split().items()})
     # energies at the converged density: E(D) with FP64 vs mixed J/K
     energies = {}
     for name, mode in (("fp64", ls.PREC_FP64), ("mixed", ls.PREC_MIXED)):
@@ -371,7 +372,12 @@ def run_ours(args):
         "roofline": {"bound": "fp64", "kernel": "k_exchange (K build, FP64)", "achieved": achieved,
                      "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
                      "peak_source": "FP64 FMA microbenchmark run in bench.py (MEASURED_PEAKS.json has no FP64 figure)",
-                     "fp32_peak": peak32},
+                     "fp32_peak": peak32,
+                     # mixed run: the pipe-bound time of its K flops, sum_prec flops_prec / peak_prec,
+                     # over the measured K time
+                     "mixed_k_frac": ((counts["mixed"]["flops_k_fp64"] / (peak64 * 1e12) +
+                                       counts["mixed"]["flops_k_fp32"] / (peak32 * 1e12)) /
+                                      (mskmx / args.steps * 1e-3))},
         "e2e": {"value": e2e_qps, "unit": "quartets/s", "h2d_bytes_per_step": nao * nao * 8,
                 "d2h_bytes_per_step": 2 * nao * nao * 8, "ms_per_step": e2e_ms / args.steps},
         "gpu_launches": int(launches_timed),

@@ -81,6 +81,12 @@ int lsjk_context_reset_stats(lsjk_context* ctx);
 /* Raw per-class quartet counters: [precision FP64, FP32][J classes (LB*5+LK),
  * K classes ((L1*3+L2)*3+L3)*3+L4]; n must be >= 2*(25+81). */
 int lsjk_context_counters(lsjk_context* ctx, unsigned long long* out, int n);
+/* Algorithmic flops of the quartets counted since the last reset, split by
+ * precision: out[0] J in FP64, out[1] J in FP32, out[2] K in FP64, out[3] K
+ * in FP32 (the per-class flop counts of lsjk_stats, by precision). For the
+ * mixed-precision roofline sum_prec flops_prec / peak_prec. No counterpart in
+ * the reference. */
+int lsjk_context_flops_split(lsjk_context* ctx, double* out4);
 
 /* Autotuner. While on, every J/K build first times candidate launch schedules
  * of each class it meets (J: ket pairs per CTA; K: CTAs per SM of each pass)

@@ -12,7 +12,7 @@ import os as _os
 from ._lightspeed import (Tensor, Primitive, Basis, Pair, PairListL, PairList, Ewald, ResourceList, IntBox,
                           PREC_MIXED, PREC_FP64, set_precision, get_precision, stats, reset_stats,
                           engine_version, stream_handle, fma_peak_tflops, coulomb_device, exchange_device,
-                          graph_begin, graph_end, Graph, class_counts, Stream,
+                          graph_begin, graph_end, Graph, class_counts, Stream, flops_split,
                           set_autotune, get_tune_table, set_tune_table)
 from .molecule import Atom, Molecule, units
 from . import gbs as _gbs

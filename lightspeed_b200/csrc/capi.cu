@@ -333,6 +333,33 @@ int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out)
     });
 }
 
+int lsjk_context_flops_split(lsjk_context* ctx, double* out4)
+{
+    return guard([&] {
+        if (!ctx || !out4) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context& c = ctx->c;
+        set_device(c);
+        std::vector<unsigned long long> h(lsjk::kNCounters);
+        LSJK_CUDA(cudaMemcpyAsync(h.data(), c.counters.p, sizeof(unsigned long long) * h.size(),
+                                  cudaMemcpyDeviceToHost, c.stream));
+        LSJK_CUDA(cudaStreamSynchronize(c.stream));
+        for (int k = 0; k < 4; ++k) out4[k] = 0.0;
+        for (int prec = 0; prec < 2; ++prec) {
+            const unsigned long long* b = h.data() + prec * (lsjk::kNJClass + lsjk::kNKClass);
+            for (int LB = 0; LB < lsjk::kNHerm; ++LB)
+                for (int LK = 0; LK < lsjk::kNHerm; ++LK)
+                    out4[prec] += (double) b[LB * lsjk::kNHerm + LK] * lsjk::j_quartet_flops(LB, LK);
+            for (int L1 = 0; L1 < lsjk::kNL; ++L1)
+                for (int L2 = 0; L2 < lsjk::kNL; ++L2)
+                    for (int L3 = 0; L3 < lsjk::kNL; ++L3)
+                        for (int L4 = 0; L4 < lsjk::kNL; ++L4) {
+                            int ci = ((L1 * lsjk::kNL + L2) * lsjk::kNL + L3) * lsjk::kNL + L4;
+                            out4[2 + prec] += (double) b[lsjk::kNJClass + ci] * lsjk::k_quartet_flops(L1, L2, L3, L4);
+                        }
+        }
+    });
+}
+
 int lsjk_context_counters(lsjk_context* ctx, unsigned long long* out, int n)
 {
     return guard([&] {

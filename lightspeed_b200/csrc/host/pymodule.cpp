@@ -196,6 +196,16 @@ PYBIND11_MODULE(_lightspeed, m)
     m.def("set_precision", [](int mode) { Engine::instance().set_precision(mode); });
     m.def("get_precision", []() { return Engine::instance().precision(); });
     m.def("stats", &stats_dict);
+    m.def("flops_split", []() {
+        double f[4];
+        check_rc(lsjk_context_flops_split(Engine::instance().ctx(), f), "flops_split");
+        py::dict d;
+        d["j_fp64"] = f[0];
+        d["j_fp32"] = f[1];
+        d["k_fp64"] = f[2];
+        d["k_fp32"] = f[3];
+        return d;
+    }, "algorithmic flops since the last reset_stats, by J/K and precision");
     m.def("class_counts", []() {
         // quartets per class: {"fp64"|"fp32": {"J": {(LB,LK): n}, "K": {(L1,L2,L3,L4): n}}}
         std::vector<unsigned long long> h(2 * (25 + 81));
