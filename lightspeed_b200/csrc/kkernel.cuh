@@ -86,9 +86,10 @@ __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const
     cp_async4(&o->c, cart + e);
 }
 
-// Densities per launch for a class: up to kKBatch while the per-density
-// registers (FP64 accumulators and the partial quartet block of N1*N3, the
-// D24 block of N2*N4, counted in 32-bit registers) stay within 64; 1 above.
+// Densities per launch for a class: up to kKBatch while a per-density
+// register weight, N1*N3*(2+w) + N2*N4*w with w the 32-bit registers of one R
+// (the segment accumulators and D24 block, with headroom for the
+// accumulation's temporaries; chosen by measurement), stays within 64; 1 above.
 template <int L1, int L2, int L3, int L4, typename R>
 __host__ __device__ constexpr int k_batch()
 {
@@ -98,15 +99,18 @@ __host__ __device__ constexpr int k_batch()
 }
 
 // One quartet (partner 1 from the staged entry e, partner 3 from registers)
-// contracted with the NG densities' D24 blocks, added to the FP64
-// accumulators. The Rys roots, weights and 1-D integrals are shared by the
-// densities (the NG inlined contractions see identical integral inputs).
+// contracted with the NG densities' D24 blocks and added straight into the
+// lane's shell-segment accumulators (type R: the FP32 pass sums the at most
+// one contracted shell's worth of quartets of a segment in FP32, and the sum
+// enters K in FP64 when the segment is flushed). The Rys roots, weights and
+// 1-D integrals are shared by the densities (the NG inlined contractions see
+// identical integral inputs).
 template <int L1, int L2, int L3, int L4, typename R, int NG>
 __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ tab, R tmax,
                                           const R* __restrict__ asym_t, const R* __restrict__ asym_w,
                                           const KEnt<R>& e, R kab34, R q, R iq, R Sx, R Sy, R Sz, R QCx,
                                           R QCy, R QCz, R Cx, R Cy, R Cz, const R (*Dblk)[ncart_of(L2) * ncart_of(L4)],
-                                          double (*acc)[ncart_of(L1) * ncart_of(L3)])
+                                          R (*acc)[ncart_of(L1) * ncart_of(L3)])
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     constexpr int N1 = ncart_of(L1), N3 = ncart_of(L3);
@@ -120,11 +124,6 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
     const R rho = p * q * ipq;
     // kab fields hold K_ab / p per pair
     const R pref = (R) kTwoPi52K * (e.kab * kab34) * rs;
-    R KV[NG][N1 * N3];
-#pragma unroll
-    for (int g = 0; g < NG; ++g)
-#pragma unroll
-        for (int t = 0; t < N1 * N3; ++t) KV[g][t] = R(0);
     for (int tm = 0; tm < A.nterm; ++tm) {
         R d2 = R(1), f = (R) A.alpha[tm] * pref;
         if (A.omega[tm] != -1.0) {
@@ -143,7 +142,7 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
 #pragma unroll
             for (int g = 0; g < NG; ++g)
                 kq_dispatch<L1, L2, L3, L4>(c00x, c00y, c00z, d00x, d00y, d00z, b00, b10, b01, e.ax, e.ay, e.az,
-                                            Cx, Cy, Cz, f * w[r], Dblk[g], KV[g]);
+                                            Cx, Cy, Cz, f * w[r], Dblk[g], acc[g]);
         };
         if constexpr (sizeof(R) == 4) {
             // FP32: roots one after another (fewer live registers, more resident warps)
@@ -154,10 +153,6 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
             for (int r = 0; r < NR; ++r) root(r);
         }
     }
-#pragma unroll
-    for (int g = 0; g < NG; ++g)
-#pragma unroll
-        for (int t = 0; t < N1 * N3; ++t) acc[g][t] += (double) KV[g][t];
 }
 
 template <int L1, int L2, int L3, int L4, typename R, int NG>
@@ -246,11 +241,11 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
             for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
             // partners 3 come by bound: no later chunk passes either
             if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
-            double acc[NG][N1 * N3];
+            R acc[NG][N1 * N3];
 #pragma unroll
             for (int g = 0; g < NG; ++g)
 #pragma unroll
-                for (int t = 0; t < N1 * N3; ++t) acc[g][t] = 0.0;
+                for (int t = 0; t < N1 * N3; ++t) acc[g][t] = R(0);
             bool any = false;
             int prev_c1 = -1;
             // flush the finished shell segment of partner 1: one atomic per element and density
@@ -265,8 +260,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                         for (int a = 0; a < N1; ++a)
 #pragma unroll
                             for (int c = 0; c < N3; ++c) {
-                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * acc[g][a * N3 + c]);
-                                acc[g][a * N3 + c] = 0.0;
+                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * (double) acc[g][a * N3 + c]);
+                                acc[g][a * N3 + c] = R(0);
                             }
                     }
                 }
