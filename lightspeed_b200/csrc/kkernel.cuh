@@ -53,6 +53,22 @@ struct alignas(16) KEnt {
     int c;
 };
 
+// Tasks a warp takes from the queue at once (at most; fewer when the class
+// has few tasks per warp, so the queue still balances the load).
+constexpr int kKGrab = 16;
+
+// Everything a task needs before its partner rows, prepared by one lane per
+// task of a grab (the loads of all the grab's tasks overlap) and read by the
+// warp as shared-memory broadcasts (64 bytes).
+struct alignas(16) KHdr {
+    double dRx, dRy, dRz;   // R2 - R4 (pair data are relative to these centres)
+    int s12, n12, s34, n34; // K-invert rows of prim2 (partners 1) and prim4 (partners 3)
+    int c2, c4;             // Cartesian offsets of prim2 and prim4
+    float tlo, thi;         // float thresholds on bound12 * bound34 for this task's max|D24|
+    float b12max;           // largest bound of the partner-1 row
+    float wsym;             // 1/2 for a diagonal task of a symmetric D24, else 1
+};
+
 // Lane l copies entry kb + l of the row (if it exists) into dst[l].
 template <typename R>
 __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const float* __restrict__ b,
@@ -145,9 +161,18 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
                                             Cx, Cy, Cz, f * w[r], Dblk[g], acc[g]);
         };
         if constexpr (sizeof(R) == 4) {
-            // FP32: roots one after another (fewer live registers, more resident warps)
+            // FP32: roots one after another (fewer live registers, more resident warps);
+            // the root in use is always slot 0 and the rest shift down, so the
+            // arrays keep static indices and stay in registers
 #pragma unroll 1
-            for (int r = 0; r < NR; ++r) root(r);
+            for (int r = 0; r < NR; ++r) {
+                root(0);
+#pragma unroll
+                for (int i = 0; i + 1 < NR; ++i) {
+                    t2[i] = t2[i + 1];
+                    w[i] = w[i + 1];
+                }
+            }
         } else {
 #pragma unroll
             for (int r = 0; r < NR; ++r) root(r);
@@ -165,6 +190,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     R* tab = reinterpret_cast<R*>(smem_raw);
     __shared__ __align__(8) uint64_t mbar;
     __shared__ KEnt<R> ring_all[kKWarps][2][32];
+    __shared__ KHdr hdr_all[kKWarps][kKGrab];
     const int ntask = *A.ntask;
     // the grid is sized for the class's task capacity; CTAs whose warps cannot
     // get a task leave before staging the quadrature table
@@ -179,141 +205,166 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     const KRows<R> d34 = [&] { if constexpr (FP64) return A.d34; else return A.f34; }();
     const int lane = threadIdx.x & 31;
     KEnt<R>* ring = &ring_all[threadIdx.x >> 5][0][0];
+    KHdr* hdr = &hdr_all[threadIdx.x >> 5][0];
     const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
     const double thr_lo = (double) A.thr_lo, thr_hi = (double) A.thr_hi;   // (float -> double exact)
+    // guided self-scheduling: a grab takes about a quarter of this warp's share of
+    // the tasks left after its previous grab (1..kKGrab), so grabs shrink to
+    // single tasks as the queue drains
+    const int nwarp4 = 4 * (int) gridDim.x * kKWarps;
+    int t0 = 0;
     long nq = 0;
     for (;;) {
-        int task = 0;
-        if (lane == 0) task = (int) atomicAdd(A.queue, 1u);
-        task = __shfl_sync(0xffffffffu, task, 0);
-        if (task >= ntask) break;
-        const KTask T = A.tasks[task];
-        const int i2 = T.i2, i4 = T.i4;
-        const double dmax = T.dmax;   // largest |D24 block| over the densities of the batch
-        // symmetric D24 (A.flip): the transposed contribution of a task with i2 != i4 is not
-        // written here; the build adds K13 to its transpose afterwards, and tasks with
-        // i2 == i4 (whose contribution is symmetric) enter with weight 1/2
-        const double wsym = (A.flip && i2 == i4) ? 0.5 : 1.0;
-        // per-task float thresholds on the bound product (exactly the double screens)
-        const float tlo = float_threshold(thr_lo, dmax);
-        const float thi = float_threshold(thr_hi, dmax);
-        // centre difference R2 - R4 (pair data are relative to these centres)
-        const R dRx = (R) (A.b2.x[i2] - A.b4.x[i4]);
-        const R dRy = (R) (A.b2.y[i2] - A.b4.y[i4]);
-        const R dRz = (R) (A.b2.z[i2] - A.b4.z[i4]);
-        const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
-        R Dblk[NG][N2 * N4];
-#pragma unroll
-        for (int g = 0; g < NG; ++g)
-#pragma unroll
-            for (int a = 0; a < N2; ++a)
-#pragma unroll
-                for (int b = 0; b < N4; ++b)
-                    Dblk[g][a * N4 + b] = (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b];
-        const int s12 = A.r12s[i2], n12 = A.r12l[i2];
-        const int s34 = A.r34s[i4], n34 = A.r34l[i4];
-        const float b12_max = A.b12[s12];   // first segment's first entry: the row maximum
-
-        for (int cs = 0; cs < n34; cs += 32) {
-            // partner 3 of this lane: entry cs + lane of the row
-            const int k3 = s34 + cs + lane;
-            bool v3 = cs + lane < n34;
-            float b34 = 0.0f;
-            if (v3) {
-                b34 = A.b34[k3];
-                v3 = b34 >= thre34;
-            }
-            R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
-            int c3 = 0;
-            if (v3) {
-                kab34 = d34.kab[k3]; q = d34.p[k3]; iq = d34.ip[k3];
-                Qx = d34.px[k3]; Qy = d34.py[k3]; Qz = d34.pz[k3];
-                Cx = d34.ax[k3]; Cy = d34.ay[k3]; Cz = d34.az[k3];
-                c3 = A.cart34[k3];
-            } else {
-                b34 = 0.0f;
-            }
-            const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
-            // ket side of PQ: (Q - R4) with the task's centre shift folded in
-            const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
-            float bmax34 = b34;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
-            // partners 3 come by bound: no later chunk passes either
-            if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
-            R acc[NG][N1 * N3];
+        const int left = ntask - t0;
+        const int grab = left >= kKGrab * nwarp4 ? kKGrab : (left >= 2 * nwarp4 ? left / nwarp4 : 1);
+        if (lane == 0) t0 = (int) atomicAdd(A.queue, (unsigned) grab);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        if (t0 >= ntask) break;
+        const int nt = min(grab, ntask - t0);
+        __syncwarp();   // the previous grab's headers have been read
+        if (lane < nt) {
+            const KTask T = A.tasks[t0 + lane];
+            const int i2 = T.i2, i4 = T.i4;
+            KHdr h;
+            h.dRx = A.b2.x[i2] - A.b4.x[i4];
+            h.dRy = A.b2.y[i2] - A.b4.y[i4];
+            h.dRz = A.b2.z[i2] - A.b4.z[i4];
+            h.s12 = A.r12s[i2];
+            h.n12 = A.r12l[i2];
+            h.s34 = A.r34s[i4];
+            h.n34 = A.r34l[i4];
+            h.c2 = A.b2.cart[i2];
+            h.c4 = A.b4.cart[i4];
+            // per-task float thresholds on the bound product (exactly the double screens);
+            // T.dmax is the largest |D24 block| over the densities of the batch
+            h.tlo = float_threshold(thr_lo, T.dmax);
+            h.thi = float_threshold(thr_hi, T.dmax);
+            h.b12max = A.b12[h.s12];   // first segment's first entry: the row maximum
+            // symmetric D24 (A.flip): the transposed contribution of a task with i2 != i4 is
+            // not written here; the build adds K13 to its transpose afterwards, and tasks with
+            // i2 == i4 (whose contribution is symmetric) enter with weight 1/2
+            h.wsym = (A.flip && i2 == i4) ? 0.5f : 1.0f;
+            hdr[lane] = h;
+        }
+        __syncwarp();
+#pragma unroll 1
+        for (int jt = 0; jt < nt; ++jt) {
+            const KHdr H = hdr[jt];
+            const double wsym = (double) H.wsym;
+            const float tlo = H.tlo, thi = H.thi;
+            const R dRx = (R) H.dRx, dRy = (R) H.dRy, dRz = (R) H.dRz;
+            const int c2 = H.c2, c4 = H.c4;
+            R Dblk[NG][N2 * N4];
 #pragma unroll
             for (int g = 0; g < NG; ++g)
 #pragma unroll
-                for (int t = 0; t < N1 * N3; ++t) acc[g][t] = R(0);
-            bool any = false;
-            int prev_c1 = -1;
-            // flush the finished shell segment of partner 1: one atomic per element and density
-            // (fire-and-forget reductions; a segmented shuffle sum over the lanes of one shell 3
-            // before them measured slower)
-            auto flush = [&]() {
-                if (any) {
+                for (int a = 0; a < N2; ++a)
 #pragma unroll
-                    for (int g = 0; g < NG; ++g) {
-                        double* Kc = A.Kc[g];
-#pragma unroll
-                        for (int a = 0; a < N1; ++a)
-#pragma unroll
-                            for (int c = 0; c < N3; ++c) {
-                                atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * (double) acc[g][a * N3 + c]);
-                                acc[g][a * N3 + c] = R(0);
-                            }
-                    }
+                    for (int b = 0; b < N4; ++b)
+                        Dblk[g][a * N4 + b] = (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b];
+            const int s12 = H.s12, n12 = H.n12;
+            const int s34 = H.s34, n34 = H.n34;
+            const float b12_max = H.b12max;
+
+            for (int cs = 0; cs < n34; cs += 32) {
+                // partner 3 of this lane: entry cs + lane of the row
+                // (all loads of the entry issue together; the bound screen applies afterwards)
+                const int k3 = s34 + cs + lane;
+                const bool in3 = cs + lane < n34;
+                float b34 = 0.0f;
+                R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
+                int c3 = 0;
+                if (in3) {
+                    b34 = A.b34[k3];
+                    kab34 = d34.kab[k3]; q = d34.p[k3]; iq = d34.ip[k3];
+                    Qx = d34.px[k3]; Qy = d34.py[k3]; Qz = d34.pz[k3];
+                    Cx = d34.ax[k3]; Cy = d34.ay[k3]; Cz = d34.az[k3];
+                    c3 = A.cart34[k3];
                 }
-                any = false;
-            };
-            stage_ent(ring, d12, A.b12, A.cart12, s12, 0, n12, lane);
-            cp_async_commit();
-            bool stop = false;
-            for (int kb = 0; kb < n12 && !stop; kb += 32) {
-                const KEnt<R>* cur = ring + ((kb >> 5) & 1) * 32;
-                if (kb + 32 < n12) stage_ent(ring + (((kb >> 5) + 1) & 1) * 32, d12, A.b12, A.cart12, s12, kb + 32, n12, lane);
-                cp_async_commit();
-                cp_async_wait<1>();
-                __syncwarp();
-                const int kend = min(32, n12 - kb);
-                // chg bit l: entry l of the chunk starts a new shell segment (l >= 1)
-                const int cl = lane < kend ? cur[lane].c : -1;
-                const int cl_prev = __shfl_up_sync(0xffffffffu, cl, 1);
-                const unsigned chg = __ballot_sync(0xffffffffu, lane >= 1 && lane < kend && cl != cl_prev);
-                for (int j = 0; j < kend; ++j) {
-                    const float b12 = cur[j].b;
-                    const int c1 = cur[j].c;
-                    if (c1 != prev_c1) {
-                        flush();
-                        prev_c1 = c1;
-                        // segments are ordered by their largest bound: nothing later passes
-                        if (b12 < thre12 || b12 * bmax34 < tlo) {
-                            stop = true;
-                            break;
+                const bool v3 = in3 && b34 >= thre34;
+                if (!v3) b34 = 0.0f;
+                const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
+                // ket side of PQ: (Q - R4) with the task's centre shift folded in
+                const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
+                float bmax34 = b34;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
+                // partners 3 come by bound: no later chunk passes either
+                if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
+                R acc[NG][N1 * N3];
+#pragma unroll
+                for (int g = 0; g < NG; ++g)
+#pragma unroll
+                    for (int t = 0; t < N1 * N3; ++t) acc[g][t] = R(0);
+                bool any = false;
+                int prev_c1 = -1;
+                // flush the finished shell segment of partner 1: one atomic per element and density
+                // (fire-and-forget reductions; a segmented shuffle sum over the lanes of one shell 3
+                // before them measured slower)
+                auto flush = [&]() {
+                    if (any) {
+#pragma unroll
+                        for (int g = 0; g < NG; ++g) {
+                            double* Kc = A.Kc[g];
+#pragma unroll
+                            for (int a = 0; a < N1; ++a)
+#pragma unroll
+                                for (int c = 0; c < N3; ++c) {
+                                    atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * (double) acc[g][a * N3 + c]);
+                                    acc[g][a * N3 + c] = R(0);
+                                }
                         }
-                    } else if (b12 < thre12 || b12 * bmax34 < tlo) {
-                        // entries of a segment are ordered by bound: skip the rest of this
-                        // segment within the chunk (to the next segment start, or the chunk end)
-                        const unsigned nxt = j == 31 ? 0u : (chg & ~((2u << j) - 1u));
-                        j = (nxt ? __ffs(nxt) - 1 : kend) - 1;
-                        continue;
                     }
-                    const float est = b12 * b34;
-                    const bool pass = v3 && est >= tlo && est < thi;
-                    if (!__any_sync(0xffffffffu, pass)) continue;
-                    if (!pass) continue;
-                    const KEnt<R> e = cur[j];
-                    ++nq;
-                    any = true;
-                    k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy, Sz, QCx,
-                                                     QCy, QCz, Cx, Cy, Cz, Dblk, acc);
+                    any = false;
+                };
+                stage_ent(ring, d12, A.b12, A.cart12, s12, 0, n12, lane);
+                cp_async_commit();
+                bool stop = false;
+                for (int kb = 0; kb < n12 && !stop; kb += 32) {
+                    const KEnt<R>* cur = ring + ((kb >> 5) & 1) * 32;
+                    if (kb + 32 < n12) stage_ent(ring + (((kb >> 5) + 1) & 1) * 32, d12, A.b12, A.cart12, s12, kb + 32, n12, lane);
+                    cp_async_commit();
+                    cp_async_wait<1>();
+                    __syncwarp();
+                    const int kend = min(32, n12 - kb);
+                    // chg bit l: entry l of the chunk starts a new shell segment (l >= 1)
+                    const int cl = lane < kend ? cur[lane].c : -1;
+                    const int cl_prev = __shfl_up_sync(0xffffffffu, cl, 1);
+                    const unsigned chg = __ballot_sync(0xffffffffu, lane >= 1 && lane < kend && cl != cl_prev);
+                    for (int j = 0; j < kend; ++j) {
+                        const float b12 = cur[j].b;
+                        const int c1 = cur[j].c;
+                        if (c1 != prev_c1) {
+                            flush();
+                            prev_c1 = c1;
+                            // segments are ordered by their largest bound: nothing later passes
+                            if (b12 < thre12 || b12 * bmax34 < tlo) {
+                                stop = true;
+                                break;
+                            }
+                        } else if (b12 < thre12 || b12 * bmax34 < tlo) {
+                            // entries of a segment are ordered by bound: skip the rest of this
+                            // segment within the chunk (to the next segment start, or the chunk end)
+                            const unsigned nxt = j == 31 ? 0u : (chg & ~((2u << j) - 1u));
+                            j = (nxt ? __ffs(nxt) - 1 : kend) - 1;
+                            continue;
+                        }
+                        const float est = b12 * b34;
+                        const bool pass = v3 && est >= tlo && est < thi;
+                        if (!__any_sync(0xffffffffu, pass)) continue;
+                        if (!pass) continue;
+                        const KEnt<R> e = cur[j];
+                        ++nq;
+                        any = true;
+                        k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy, Sz, QCx,
+                                                         QCy, QCz, Cx, Cy, Cz, Dblk, acc);
+                    }
+                    __syncwarp();   // the next chunk's prefetch refills this slot
                 }
-                __syncwarp();   // the next chunk's prefetch refills this slot
+                cp_async_wait<0>();
+                __syncwarp();
+                flush();
             }
-            cp_async_wait<0>();
-            __syncwarp();
-            flush();
         }
     }
     for (int o = 16; o > 0; o >>= 1) nq += __shfl_xor_sync(0xffffffffu, nq, o);
