@@ -7,8 +7,8 @@ mixed-precision cutoff thredp = 1e-5) on the converged RHF density of all-trans
 C40H82 in cc-pVDZ (970 pure / 1010 Cartesian functions, 1290 primitive
 shells). `value` is quartets/s with D, J and K resident in HBM (device entry
 points); `e2e` is the same metric through the public host API
-(ls.IntBox.coulomb / exchange on host tensors: the H2D copy of D and the D2H
-copies of J and K are inside the timed region). L2 is flushed between steps
+(ls.IntBox.coulomb / exchange on host tensors: each call's H2D copy of D and
+the D2H copies of J and K are inside the timed region). L2 is flushed between steps
 by writing a 256 MiB buffer outside the timed events. For N > 1 each rank
 runs an independent replica on its own GPU (weak scaling); the max time over
 ranks is used. `--impl reference` times the reference CPU IntBox
