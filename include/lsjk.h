@@ -187,6 +187,23 @@ int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const double* scal
                                 const lsjk_pairlist* pl12, const lsjk_pairlist* pl34,
                                 const double* D34_dev, float thresp, float thredp, double* J12_dev);
 
+/* Two-electron integrals in an MO basis through J builds: for host
+ * coefficient blocks C1 (nao1 x n1), C2 (nao2 x n2), C3 (nao3 x n3),
+ * C4 (nao4 x n4), row-major, with nao1/nao2 the bases of pl12 and nao3/nao4
+ * those of pl34, writes (overwrites) I[i][j][k][l] = (C1_i C2_j | C3_k C4_l)
+ * (host, n1*n2*n3*n4 doubles). Replaces IntBox::eriJ
+ * (src/cpp/intbox/mo_eri.cpp:10-157): one J build per (i, j), with i >= j
+ * when sym12, of the density C1[:,i] C2[:,j]^T over pl34's pairs (bra pl34,
+ * ket pl12, mo_eri.cpp:74-118), then I[i][j] = C3^T J C4. Here the densities
+ * are formed on the device and go through the batched J path 16 at a time;
+ * J never leaves the device. The flags stand for the reference's
+ * pointer-identity tests and select its symmetrisations (mo_eri.cpp:121-155):
+ * sym12 for C1 == C2, sym34 for C3 == C4, sym1234 for C1 == C3 and C2 == C4. */
+int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+               const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int n1, int n2, int n3, int n4,
+               const double* C1, const double* C2, const double* C3, const double* C4, int sym12, int sym34,
+               int sym1234, float thresp, float thredp, double* I);
+
 /* ---- CUDA graphs: capture the builds issued through the *_device entry
  * points between lsjk_graph_begin and lsjk_graph_end on the context stream,
  * then replay them with one lsjk_graph_launch (an SCF iteration's J+K as one

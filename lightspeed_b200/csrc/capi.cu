@@ -793,3 +793,170 @@ extern "C" int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const d
         }
     });
 }
+
+// ---- MO-basis integrals through J builds (IntBox::eriJ, src/cpp/intbox/mo_eri.cpp:10-157)
+
+namespace {
+
+constexpr int kEriBatch = 16;   // (i, j) densities per round of J builds
+
+struct EriPairs {
+    int i[kEriBatch], j[kEriBatch];
+};
+
+// D[g] = C1[:, i_g] C2[:, j_g]^T (nao1 x nao2, row-major; mo_eri.cpp:75-86)
+__global__ void k_eri_density(EriPairs P, int ng, const double* __restrict__ C1, int n1,
+                              const double* __restrict__ C2, int n2, int nao1, int nao2, double* __restrict__ D)
+{
+    const long per = (long) nao1 * nao2, total = per * ng;
+    for (long t = blockIdx.x * (long) blockDim.x + threadIdx.x; t < total; t += (long) gridDim.x * blockDim.x) {
+        const int g = (int) (t / per);
+        const long pq = t - g * per;
+        const int p = (int) (pq / nao2), q = (int) (pq - (long) p * nao2);
+        D[t] = C1[(long) p * n1 + P.i[g]] * C2[(long) q * n2 + P.j[g]];
+    }
+}
+
+// T[g][k][s] = sum_r C3[r][k] J[g][r][s]; grid (s blocks, k, g)
+__global__ void k_eri_left(int nao3, int nao4, int n3, const double* __restrict__ C3, const double* __restrict__ J,
+                           double* __restrict__ T)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y, g = blockIdx.z;
+    if (s >= nao4) return;
+    const double* Jg = J + (long) g * nao3 * nao4;
+    double acc = 0.0;
+    for (int r = 0; r < nao3; ++r) acc += C3[(long) r * n3 + k] * Jg[(long) r * nao4 + s];
+    T[((long) g * n3 + k) * nao4 + s] = acc;
+}
+
+// I[i_g][j_g][k][l] = sum_s T[g][k][s] C4[s][l], also stored at I[j_g][i_g] for
+// a symmetric pair (mo_eri.cpp:112-116)
+__global__ void k_eri_right(EriPairs P, int ng, int n2, int n3, int n4, int nao4, const double* __restrict__ T,
+                            const double* __restrict__ C4, int sym12, double* __restrict__ I)
+{
+    const long n34 = (long) n3 * n4, total = ng * n34;
+    for (long t = blockIdx.x * (long) blockDim.x + threadIdx.x; t < total; t += (long) gridDim.x * blockDim.x) {
+        const int g = (int) (t / n34);
+        const int kl = (int) (t - g * n34);
+        const int k = kl / n4, l = kl - k * n4;
+        const double* Tk = T + ((long) g * n3 + k) * nao4;
+        double acc = 0.0;
+        for (int s = 0; s < nao4; ++s) acc += Tk[s] * C4[(long) s * n4 + l];
+        I[((long) P.i[g] * n2 + P.j[g]) * n34 + kl] = acc;
+        if (sym12 && P.i[g] != P.j[g]) I[((long) P.j[g] * n2 + P.i[g]) * n34 + kl] = acc;
+    }
+}
+
+void upload(lsjk::DBuf<double>& d, const double* h, size_t n, cudaStream_t s)
+{
+    d.alloc(n);
+    if (n) LSJK_CUDA(cudaMemcpyAsync(d.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+}
+
+} // namespace
+
+extern "C" int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                          const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int n1, int n2, int n3, int n4,
+                          const double* C1, const double* C2, const double* C3, const double* C4, int sym12,
+                          int sym34, int sym1234, float thresp, float thredp, double* I)
+{
+    return guard([&] {
+        if (!ctx || !pl12 || !pl34) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        if (n1 < 0 || n2 < 0 || n3 < 0 || n4 < 0) throw lsjk::Error(LSJK_EINVAL, "negative orbital count");
+        if ((sym12 && n1 != n2) || (sym34 && n3 != n4) || (sym1234 && (n1 != n3 || n2 != n4)))
+            throw lsjk::Error(LSJK_EINVAL, "a symmetry flag needs equal orbital counts");
+        const size_t nI = (size_t) n1 * n2 * n3 * n4;
+        if (nI && (!C1 || !C2 || !C3 || !C4 || !I)) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        check_lmax(&pl12->p);
+        check_lmax(&pl34->p);
+        if (!nI) return;
+        const int nao1 = pl12->p.b1->nao, nao2 = pl12->p.b2->nao;
+        const int nao3 = pl34->p.b1->nao, nao4 = pl34->p.b2->nao;
+        cudaStream_t s = c->stream;
+        lsjk::DBuf<double> dC1, dC2, dC3, dC4, dD, dJ, dT, dI;
+        upload(dC1, C1, (size_t) nao1 * n1, s);
+        upload(dC2, C2, (size_t) nao2 * n2, s);
+        upload(dC3, C3, (size_t) nao3 * n3, s);
+        upload(dC4, C4, (size_t) nao4 * n4, s);
+        const size_t n12 = (size_t) nao1 * nao2, n34 = (size_t) nao3 * nao4;
+        dD.alloc(n12 * kEriBatch);
+        dJ.alloc(n34 * kEriBatch);
+        dT.alloc((size_t) kEriBatch * n3 * nao4);
+        dI.alloc(nI);
+        // the (i, j) densities, i >= j when the bra is symmetric (mo_eri.cpp:71-74)
+        std::vector<std::pair<int, int>> ij;
+        for (int i = 0; i < n1; ++i)
+            for (int j = 0; j < n2; ++j)
+                if (!(sym12 && i < j)) ij.emplace_back(i, j);
+        for (size_t b0 = 0; b0 < ij.size(); b0 += kEriBatch) {
+            const int ng = (int) std::min<size_t>(kEriBatch, ij.size() - b0);
+            EriPairs P{};
+            for (int g = 0; g < ng; ++g) {
+                P.i[g] = ij[b0 + g].first;
+                P.j[g] = ij[b0 + g].second;
+            }
+            if (n12) {
+                const long tot = (long) n12 * ng;
+                k_eri_density<<<(unsigned) std::min<long>((tot + 255) / 256, 4096), 256, 0, s>>>(
+                    P, ng, dC1.p, n1, dC2.p, n2, nao1, nao2, dD.p);
+                LSJK_CUDA(cudaGetLastError());
+            }
+            if (n34) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * n34 * ng, s));
+            // J over pl34's pairs of each density on pl12's bases (bra pl34, ket pl12: mo_eri.cpp:88-95)
+            for (int g0 = 0; g0 < ng; g0 += lsjk::kJBatchMax) {
+                const int m = std::min(lsjk::kJBatchMax, ng - g0);
+                const double* dp[lsjk::kJBatchMax];
+                double* jp[lsjk::kJBatchMax];
+                for (int g = 0; g < m; ++g) {
+                    dp[g] = dD.p + (g0 + g) * n12;
+                    jp[g] = dJ.p + (g0 + g) * n34;
+                }
+                coulomb_group(c, ew, &pl34->p, &pl12->p, dp, jp, m, thresp, thredp);
+            }
+            // L = C3^T J C4 (mo_eri.cpp:96-110)
+            if (nao4 > 0 && nao3 > 0) {
+                k_eri_left<<<dim3((unsigned) ((nao4 + 127) / 128), (unsigned) n3, (unsigned) ng), 128, 0, s>>>(
+                    nao3, nao4, n3, dC3.p, dJ.p, dT.p);
+                LSJK_CUDA(cudaGetLastError());
+            } else if (nao4 > 0) {
+                LSJK_CUDA(cudaMemsetAsync(dT.p, 0, sizeof(double) * ng * n3 * (size_t) nao4, s));
+            }
+            const long tot = (long) ng * n3 * n4;
+            k_eri_right<<<(unsigned) std::min<long>((tot + 127) / 128, 4096), 128, 0, s>>>(
+                P, ng, n2, n3, n4, nao4, dT.p, dC4.p, sym12, dI.p);
+            LSJK_CUDA(cudaGetLastError());
+        }
+        LSJK_CUDA(cudaMemcpyAsync(I, dI.p, sizeof(double) * nI, cudaMemcpyDeviceToHost, s));
+        check_kernels(c);
+        // the reference's symmetrisations, in its order (mo_eri.cpp:121-155)
+        const size_t s234 = (size_t) n2 * n3 * n4, s34 = (size_t) n3 * n4;
+        if (sym12)
+            for (size_t rs = 0; rs < s34; ++rs)
+                for (int p = 0; p < n1; ++p)
+                    for (int q = 0; q < p; ++q) {
+                        double& a = I[p * s234 + q * s34 + rs];
+                        double& b = I[q * s234 + p * s34 + rs];
+                        a = b = 0.5 * (a + b);
+                    }
+        if (sym34)
+            for (size_t pq = 0; pq < (size_t) n1 * n2; ++pq) {
+                double* Ip = I + pq * s34;
+                for (int r = 0; r < n3; ++r)
+                    for (int t = 0; t < r; ++t) {
+                        double& a = Ip[r * n4 + t];
+                        double& b = Ip[t * n4 + r];
+                        a = b = 0.5 * (a + b);
+                    }
+            }
+        if (sym1234)
+            for (size_t pq = 0; pq < (size_t) n1 * n2; ++pq)
+                for (size_t rs = 0; rs < pq; ++rs) {
+                    double& a = I[pq * s34 + rs];
+                    double& b = I[rs * s34 + pq];
+                    a = b = 0.5 * (a + b);
+                }
+    });
+}

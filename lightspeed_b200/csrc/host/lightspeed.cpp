@@ -361,4 +361,34 @@ std::vector<std::shared_ptr<Tensor>> IntBox::exchangeMulti(
     return out;
 }
 
+std::shared_ptr<Tensor> IntBox::eriJ(const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ewald,
+                                     const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,
+                                     const std::shared_ptr<Tensor>& C1, const std::shared_ptr<Tensor>& C2,
+                                     const std::shared_ptr<Tensor>& C3, const std::shared_ptr<Tensor>& C4,
+                                     float thresp, float thredp, const std::shared_ptr<Tensor>& I)
+{
+    const std::shared_ptr<Tensor>* C[4] = {&C1, &C2, &C3, &C4};
+    const size_t nao[4] = {pl12->basis1()->nao(), pl12->basis2()->nao(), pl34->basis1()->nao(),
+                           pl34->basis2()->nao()};
+    size_t n[4];
+    for (int a = 0; a < 4; ++a) {
+        if (!*C[a]) throw std::runtime_error("IntBox::eriJ: null coefficient tensor");
+        (*C[a])->ndim_error(2);
+        n[a] = (*C[a])->shape()[1];
+        (*C[a])->shape_error({nao[a], n[a]});
+    }
+    std::shared_ptr<Tensor> out = I;
+    if (out)
+        out->shape_error({n[0], n[1], n[2], n[3]});
+    else
+        out = std::make_shared<Tensor>(std::vector<size_t>{n[0], n[1], n[2], n[3]}, "I");
+    check_rc(lsjk_eri_j(Engine::instance().ctx(), (int) ewald->scales().size(), ewald->scales().data(),
+                        ewald->omegas().data(), pl12->device_handle(), pl34->device_handle(), (int) n[0], (int) n[1],
+                        (int) n[2], (int) n[3], C1->data().data(), C2->data().data(), C3->data().data(),
+                        C4->data().data(), C1 == C2 ? 1 : 0, C3 == C4 ? 1 : 0, (C1 == C3 && C2 == C4) ? 1 : 0,
+                        thresp, thredp, out->data().data()),
+             "IntBox::eriJ");
+    return out;
+}
+
 } // namespace lightspeed

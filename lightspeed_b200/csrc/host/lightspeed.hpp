@@ -7,6 +7,7 @@
 //   Ewald         src/lightspeed/ewald.hpp:25-109
 //   ResourceList  src/lightspeed/resource_list.hpp:25-73
 //   IntBox::coulomb/exchange  src/lightspeed/intbox.hpp:761-771, 817-828
+//   IntBox::eriJ  src/lightspeed/intbox.hpp:1349, src/cpp/intbox/mo_eri.cpp:10-157
 // The integral work goes through the C ABI in include/lsjk.h (liblsjk.so);
 // nothing here computes J or K on the CPU.
 #pragma once
@@ -221,6 +222,17 @@ public:
         const std::shared_ptr<PairList>& pairlist12, const std::shared_ptr<PairList>& pairlist34,
         const std::vector<std::shared_ptr<Tensor>>& D24, bool D24symm, float thresp, float thredp,
         const std::vector<std::shared_ptr<Tensor>>& K13 = {});
+    // (C1_i C2_j | C3_k C4_l) through J builds (mo_eri.cpp:10-157); the
+    // symmetrisations follow the reference's tests of object identity
+    // (C1 is C2, C3 is C4, C1 is C3 and C2 is C4).
+    static std::shared_ptr<Tensor> eriJ(const std::shared_ptr<ResourceList>& resources,
+                                        const std::shared_ptr<Ewald>& ewald,
+                                        const std::shared_ptr<PairList>& pairlist12,
+                                        const std::shared_ptr<PairList>& pairlist34,
+                                        const std::shared_ptr<Tensor>& C1, const std::shared_ptr<Tensor>& C2,
+                                        const std::shared_ptr<Tensor>& C3, const std::shared_ptr<Tensor>& C4,
+                                        float thresp, float thredp,
+                                        const std::shared_ptr<Tensor>& I = std::shared_ptr<Tensor>());
 };
 
 // Raise std::runtime_error with the engine's message when rc != 0.

@@ -176,6 +176,10 @@ PYBIND11_MODULE(_lightspeed, m)
                     py::arg("pairlist12"), py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"),
                     py::arg("thresp"), py::arg("thredp"), py::arg("K13") = std::vector<std::shared_ptr<Tensor>>(),
                     py::call_guard<py::gil_scoped_release>())
+        .def_static("eriJ", &IntBox::eriJ, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
+                    py::arg("pairlist34"), py::arg("C1"), py::arg("C2"), py::arg("C3"), py::arg("C4"),
+                    py::arg("thresp"), py::arg("thredp"), py::arg("I") = std::shared_ptr<Tensor>(),
+                    py::call_guard<py::gil_scoped_release>())
         // one-electron integrals for the SCF drivers (host C++)
         .def_static("overlap", [](const std::shared_ptr<ResourceList>&, const std::shared_ptr<PairList>& pl,
                                   const std::shared_ptr<Tensor>& S) { return OneInt::overlap(pl, S); },

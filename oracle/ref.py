@@ -145,3 +145,37 @@ def rys(nrys, T):
     w = np.zeros((len(T), nrys))
     _check(lib().ref_rys(nrys, len(T), _p(T), _p(t), _p(w)))
     return t, w
+
+
+def eri_j(pl12, pl34, C1, C2, C3, C4, thresp, thredp, sym12, sym34, sym1234, scales=(1.0,), omegas=(-1.0,)):
+    """IntBox::eriJ restated over the reference's own CPU coulomb
+    (src/cpp/intbox/mo_eri.cpp:10-157): one J build per (i, j) (i >= j when
+    sym12) of D = C1[:, i] C2[:, j]^T with bra pl34 and ket pl12 (:74-95),
+    I[i, j] = C3^T J C4 (:96-118), then the symmetrisations of :121-155 in
+    that order; the flags stand for its object-identity tests."""
+    n1, n2, n3, n4 = C1.shape[1], C2.shape[1], C3.shape[1], C4.shape[1]
+    I = np.zeros((n1, n2, n3, n4))
+    for i in range(n1):
+        for j in range(n2):
+            if sym12 and i < j:
+                continue
+            D = np.outer(C1[:, i], C2[:, j])
+            J = coulomb(pl34, pl12, D, thresp, thredp, scales, omegas)
+            L = C3.T @ J @ C4
+            I[i, j] = L
+            if sym12 and i != j:
+                I[j, i] = L
+    if sym12:
+        for p in range(n1):
+            for q in range(p):
+                I[p, q] = I[q, p] = 0.5 * (I[p, q] + I[q, p])
+    if sym34:
+        for r in range(n3):
+            for s in range(r):
+                I[:, :, r, s] = I[:, :, s, r] = 0.5 * (I[:, :, r, s] + I[:, :, s, r])
+    if sym1234:
+        M = I.reshape(n1 * n2, n3 * n4)
+        for pq in range(n1 * n2):
+            for rs in range(pq):
+                M[pq, rs] = M[rs, pq] = 0.5 * (M[pq, rs] + M[rs, pq])
+    return I
