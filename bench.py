@@ -41,11 +41,13 @@ def parse():
     ap.add_argument("--carbons", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scf-maxiter", type=int, default=60)
-    ap.add_argument("--workload", default="alkane", choices=["alkane", "batched", "guess", "many"],
+    ap.add_argument("--workload", default="alkane", choices=["alkane", "batched", "guess", "many", "eri"],
                     help="alkane: the headline C40H82 J+K step; batched: 64 response-like densities "
                          "of a 32-water cluster per step (one line per operator and precision); guess: "
                          "train the learned SCF guess and time SCFs from it against SAD")
     ap.add_argument("--molecules", type=int, default=512, help="many: number of water clusters")
+    ap.add_argument("--waters", type=int, default=16, help="eri: water cluster size")
+    ap.add_argument("--active", type=int, default=12, help="eri: active orbitals")
     ap.add_argument("--train-clusters", type=int, default=1000)
     ap.add_argument("--test-clusters", type=int, default=20)
     ap.add_argument("--epochs", type=int, default=40)
@@ -575,6 +577,68 @@ def run_guess(args):
     return 0
 
 
+def run_eri(args):
+    """MO-basis integrals through J builds (IntBox.eriJ, the CASCI integrals):
+    a `--waters` H2O cluster (seed 0) in 6-31G*, Schwarz 1e-12, one block of
+    `--active` S-orthonormal orbitals (seeded) passed as all four coefficient
+    tensors, so n(n+1)/2 J builds per call. A step is one IntBox.eriJ call
+    through the host API (C in, I out, both host arrays), timed on the wall
+    clock around the synchronous call; FP64 and mixed. `value` = J builds per
+    second in FP64 (the faster mode here); the mixed integrals are compared
+    with FP64 elementwise. Beside it, the reference's structure on the same
+    engine: one host IntBox.coulomb call per (i, j) and a host contraction."""
+    rank, world, local = dist_info()
+    import torch
+    torch.cuda.set_device(local)
+    import lightspeed_b200 as ls
+    from lightspeed_b200.geometry import water_cluster
+    mol = water_cluster(args.waters, seed=0)
+    bas = ls.Basis.from_gbs_file(mol, "6-31gs")
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1.0e-12)
+    S = ls.IntBox.overlap(res, pl).np.copy()
+    X = np.random.default_rng(0).standard_normal((bas.nao, args.active))
+    w, V = np.linalg.eigh(X.T @ S @ X)
+    C = ls.Tensor.array(X @ V / np.sqrt(w))
+    ew = ls.Ewald.coulomb()
+    nbuild = args.active * (args.active + 1) // 2
+    out = {}
+    for name, prec in (("fp64", ls.PREC_FP64), ("mixed", ls.PREC_MIXED)):
+        ls.set_precision(prec)
+        for _ in range(args.warmup):
+            ls.IntBox.eriJ(res, ew, pl, pl, C, C, C, C, THRE, THREDP)
+        t = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            I = ls.IntBox.eriJ(res, ew, pl, pl, C, C, C, C, THRE, THREDP)
+            t.append(time.perf_counter() - t0)
+        out[name] = {"ms_per_call": 1e3 * float(np.mean(t)), "builds_per_s": nbuild / float(np.mean(t)),
+                     "I": I.np.copy()}
+    # the reference's structure on the same engine: one host J call per (i, j) and a host contraction
+    ls.set_precision(ls.PREC_FP64)
+    Cn = C.np
+    t0 = time.perf_counter()
+    for i in range(args.active):
+        for j in range(i + 1):
+            J = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(np.outer(Cn[:, i], Cn[:, j])), THRE, THREDP).np
+            Cn.T @ J @ Cn
+    out["fp64"]["host_loop_ms"] = 1e3 * (time.perf_counter() - t0)
+    ls.set_precision(ls.PREC_MIXED)
+    err = float(np.max(np.abs(out["mixed"]["I"] - out["fp64"]["I"])))
+    for v in out.values():
+        del v["I"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": "IntBox.eriJ J builds per second (CASCI active-space integrals)",
+            "value": out["fp64"]["builds_per_s"], "unit": "J builds/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["fp64"]["ms_per_call"], "higher_is_better": True,
+            "data": "synthetic", "dtype": "f64",
+            "config": {"workload": "eriJ", "waters": args.waters, "basis": "6-31G*", "nao": bas.nao,
+                       "active": args.active, "j_builds_per_call": nbuild, "thresp": THRE, "thredp": THREDP},
+            "fp64": out["fp64"], "mixed": out["mixed"], "max_abs_dI_mixed_vs_fp64": err}))
+    return 0
+
+
 def run_many(args):
     """Many-molecule batch: `--molecules` seeded water clusters of 1-12 H2O
     (sizes from default_rng(0), cluster m from seed m), 6-31G*, FP64 J/K,
@@ -779,6 +843,8 @@ def main():
         return run_guess(args)
     if args.workload == "many":
         return run_many(args)
+    if args.workload == "eri":
+        return run_eri(args)
     return run_ours(args)
 
 
