@@ -29,6 +29,7 @@ sys.path.insert(0, ROOT)
 METRIC = "J+K ms/iter & quartets/s: mixed vs FP64 GPU at |ΔE|≤1e-6 Eh; CPU ref alongside"
 THRE = 1.0e-14
 THREDP = 1.0e-5
+K_TRAFFIC_C40 = 5.154e9   # ncu dram__bytes_read.sum + dram__bytes_write.sum, FP64 K build of C40H82
 SAMPLE_CARBONS = 8        # CPU baseline sample: C8H18 / cc-pVDZ, full J+K
 
 
@@ -372,7 +373,12 @@ def run_ours(args):
                   "quartets_fp32": counts["mixed"]["quartets_fp32"], "quartets": qmx,
                   "speedup_vs_fp64": ms64 / msmx, "dE_vs_fp64_Eh": dE},
         "roofline": {"bound": "fp64", "kernel": "k_exchange (K build, FP64)", "achieved": achieved,
-                     "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64, "traffic": None,
+                     "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                     # DRAM bytes (read + write) of the FP64 K build's 81 launches of this workload,
+                     # from one ncu capture (cold cache per launch: an upper bound)
+                     "traffic": K_TRAFFIC_C40 if args.carbons == 40 else None,
+                     "traffic_unit": "bytes per FP64 K build",
+                     "traffic_source": "profiles/dram_jk_C40H82_ccpvdz.md",
                      "peak_source": "FP64 FMA microbenchmark run in bench.py (MEASURED_PEAKS.json has no FP64 figure)",
                      "fp32_peak": peak32,
                      # mixed run: the pipe-bound time of its K flops, sum_prec flops_prec / peak_prec,
