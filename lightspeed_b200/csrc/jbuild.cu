@@ -215,6 +215,39 @@ __global__ void k_ket_bounds(const unsigned* __restrict__ keys_sorted, const int
 
 // ---- 5. bra Hermite -> Cartesian --------------------------------------------
 
+// Hermite index t -> (tx, ty, tz) as a compile-time table (so unrolled loops
+// index registers, not memory).
+struct HermTab {
+    int x[35], y[35], z[35];
+};
+__host__ __device__ constexpr HermTab make_herm_tab()
+{
+    HermTab T{};
+    for (int t = 0; t < 35; ++t) {
+        T.x[t] = herm_tx(t);
+        T.y[t] = herm_ty(t);
+        T.z[t] = herm_tz(t);
+    }
+    return T;
+}
+
+// Cartesian exponents (lx, ly, lz) of component k of a shell of angular
+// momentum L <= 2, as a compile-time table.
+struct CartTab {
+    int x[3][6], y[3][6], z[3][6];
+};
+__host__ __device__ constexpr CartTab make_cart_tab()
+{
+    CartTab T{};
+    for (int L = 0; L <= 2; ++L)
+        for (int k = 0; k < ncart_of(L); ++k) {
+            T.x[L][k] = cart_lx(L, k);
+            T.y[L][k] = cart_ly(L, k);
+            T.z[L][k] = cart_lz(L, k);
+        }
+    return T;
+}
+
 template <int L1, int L2>
 __device__ void bra_to_cart(int i, int j, BasisView b1, BasisView b2, bool symm, const double* __restrict__ geom,
                             const double* __restrict__ jt, double* __restrict__ Jc)
@@ -242,12 +275,14 @@ __device__ void bra_to_cart(int i, int j, BasisView b1, BasisView b2, bool symm,
     for (int x = 0; x < N1; ++x)
 #pragma unroll
         for (int y = 0; y < N2; ++y) {
+            constexpr HermTab ht = make_herm_tab();
+            constexpr CartTab ct = make_cart_tab();
             double s = 0.0;
 #pragma unroll
             for (int t = 0; t < H; ++t)
-                s += E.v[0][cart_lx(L1, x)][cart_lx(L2, y)][herm_tx(t)] *
-                     E.v[1][cart_ly(L1, x)][cart_ly(L2, y)][herm_ty(t)] *
-                     E.v[2][cart_lz(L1, x)][cart_lz(L2, y)][herm_tz(t)] * jt[t];
+                s += E.v[0][ct.x[L1][x]][ct.x[L2][y]][ht.x[t]] *
+                     E.v[1][ct.y[L1][x]][ct.y[L2][y]][ht.y[t]] *
+                     E.v[2][ct.z[L1][x]][ct.z[L2][y]][ht.z[t]] * jt[t];
             s *= pre;
             atomicAdd(&Jc[(long) (a1 + x) * ld + a2 + y], s);
             if (symm) atomicAdd(&Jc[(long) (a2 + y) * ld + a1 + x], s);
@@ -275,6 +310,82 @@ __global__ void k_herm_to_cart(const int* __restrict__ nbra, const int* __restri
         else bra_to_cart<0, 2>(i, j, b1, b2, symm, g, jt, Jc);
     } else if (LB == 3) { if (L1 == 2) bra_to_cart<2, 1>(i, j, b1, b2, symm, g, jt, Jc); else bra_to_cart<1, 2>(i, j, b1, b2, symm, g, jt, Jc); }
     else bra_to_cart<2, 2>(i, j, b1, b2, symm, g, jt, Jc);
+}
+
+// The same transform for the high bra classes (LB >= 3), a warp per bra
+// pair: lane o (and o + 32) owns the Cartesian output (x, y) = (o / N2, o % N2)
+// and raises its three 1-D coefficient vectors E^{l1,l2}_t in registers by the
+// recursion of build_E (first in the exponent on A, then on B), so no
+// coefficient table goes to local memory (one thread per pair needs the whole
+// (LA+1)(LB+1)(LA+LB+1) table per direction).
+template <int LB>
+__global__ void k_herm_to_cart_warp(const int* __restrict__ nbra, const int* __restrict__ p1,
+                                    const int* __restrict__ p2, const double* __restrict__ geom,
+                                    BasisView b1, BasisView b2, int symm, const double* __restrict__ jbra,
+                                    double* __restrict__ Jc)
+{
+    constexpr int H = nherm_of(LB), V = LB + 1;
+    const int lane = threadIdx.x & 31;
+    const long k = ((long) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= *nbra) return;   // whole warps leave together
+    const int i = p1[k], j = p2[k];
+    const int L1 = b1.L[i], L2 = LB - L1;
+    const int N1 = ncart_of(L1), N2 = ncart_of(L2);
+    const double* g = geom + 4L * k;
+    const double p = g[0];
+    const double A[3] = {b1.x[i], b1.y[i], b1.z[i]};
+    const double B[3] = {b2.x[j], b2.y[j], b2.z[j]};
+    double PA[3], PB[3];
+    double R2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        PA[d] = g[1 + d] - A[d];
+        PB[d] = g[1 + d] - B[d];
+        R2 += (A[d] - B[d]) * (A[d] - B[d]);
+    }
+    double pre = kTwoPi52 / p * b1.c[i] * b2.c[j] * exp(-b1.e[i] * b2.e[j] / p * R2);
+    if (symm && i == j) pre *= 0.5;
+    const double h = 0.5 / p;
+    const double* jt = jbra + k * H;
+    const int a1 = b1.cart[i], a2 = b2.cart[j], ld = b2.ncart;
+    struct Ev {
+        double v[V];
+    };
+    // E^{l1,l2}_t of one direction: raised n1 times on A, then n2 times on B,
+    // each step E'_t = X E_t + h E_{t-1} + (t+1) E_{t+1}
+    auto vec = [h](int n1, int n2, double XA, double XB) {
+        Ev e;
+#pragma unroll
+        for (int t = 0; t < V; ++t) e.v[t] = t == 0 ? 1.0 : 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            if (r >= n1 + n2) break;
+            const double X = r < n1 ? XA : XB;
+            Ev n;
+#pragma unroll
+            for (int t = 0; t < V; ++t) {
+                double s = X * e.v[t];
+                if (t > 0) s += h * e.v[t - 1];
+                if (t + 1 < V) s += (t + 1) * e.v[t + 1];
+                n.v[t] = s;
+            }
+            e = n;
+        }
+        return e;
+    };
+    for (int o = lane; o < N1 * N2; o += 32) {
+        const int x = o / N2, y = o - x * N2;
+        const Ev ex = vec(cart_lx(L1, x), cart_lx(L2, y), PA[0], PB[0]);
+        const Ev ey = vec(cart_ly(L1, x), cart_ly(L2, y), PA[1], PB[1]);
+        const Ev ez = vec(cart_lz(L1, x), cart_lz(L2, y), PA[2], PB[2]);
+        constexpr HermTab ht = make_herm_tab();
+        double s = 0.0;
+#pragma unroll
+        for (int t = 0; t < H; ++t) s += ex.v[ht.x[t]] * ey.v[ht.y[t]] * ez.v[ht.z[t]] * jt[t];
+        s *= pre;
+        atomicAdd(&Jc[(long) (a1 + x) * ld + a2 + y], s);
+        if (symm) atomicAdd(&Jc[(long) (a2 + y) * ld + a1 + x], s);
+    }
 }
 
 template <int LB>
@@ -478,8 +589,8 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             case 0: k_herm_to_cart<0><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
             case 1: k_herm_to_cart<1><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
             case 2: k_herm_to_cart<2><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
-            case 3: k_herm_to_cart<3><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
-            case 4: k_herm_to_cart<4><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 3: k_herm_to_cart_warp<3><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 4: k_herm_to_cart_warp<4><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
             }
             LSJK_CUDA(cudaGetLastError());
             ctx->stats.kernel_launches++;
