@@ -98,48 +98,70 @@ struct TaskGenArgs {
     int split;
 };
 
+// Append one task per lane that wants one to the list of its class c: the
+// lanes of the warp with the same class take consecutive slots from one
+// atomic (the leader's), so the per-class counters see one atomic per warp
+// and class instead of one per task.
+__device__ __forceinline__ void append_task(unsigned want_mask, int c, long off, int* __restrict__ count,
+                                            KTask* __restrict__ list, const KTask& t)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(want_mask, c);
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&count[c], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    list[off + base + __popc(peers & ((1u << lane) - 1u))] = t;
+}
+
 __global__ void k_task_gen(TaskGenArgs A)
 {
-    int i2 = blockIdx.y;
-    int i4 = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i4 >= A.b4.nprim) return;
-    if (A.d24symm && i2 > i4) return;   // exchange.cpp:137-139
+    const int i2 = blockIdx.y;
+    const int i4 = blockIdx.x * blockDim.x + threadIdx.x;
+    // exchange.cpp:137-139 (prim2 <= prim4 for a symmetric D24); lanes out of
+    // range stay for the warp-wide votes below
+    const bool valid = i4 < A.b4.nprim && !(A.d24symm && i2 > i4);
+    if (!__any_sync(0xffffffffu, valid)) return;
     const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
-    int L2 = A.b2.L[i2], L4 = A.b4.L[i4];
-    int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
-    int n2 = ncart_of(L2), n4 = ncart_of(L4);
+    const int L2 = A.b2.L[i2];
+    const int L4 = valid ? A.b4.L[i4] : 0;
     // largest |D24| over the pair's block and the batch's densities
     double dmax = 0.0;
-    for (int g = 0; g < A.ng; ++g)
-        for (int a = 0; a < n2; ++a)
-            for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b]));
+    if (valid) {
+        const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
+        const int n2 = ncart_of(L2), n4 = ncart_of(L4);
+        for (int g = 0; g < A.ng; ++g)
+            for (int a = 0; a < n2; ++a)
+                for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b]));
+    }
     for (int L1 = 0; L1 < kNL; ++L1) {
         const int* rl12 = A.r12.len[L2][L1];
+        // uniform over the block (i2 and L2 are)
         if (!rl12) continue;
-        int len12 = rl12[i2];
+        const int len12 = rl12[i2];
         if (!len12) continue;
-        float b12 = A.pb12[A.r12.start[L2][L1][i2]];
+        const float b12 = A.pb12[A.r12.start[L2][L1][i2]];
         if (b12 < thre12) continue;
         for (int L3 = 0; L3 < kNL; ++L3) {
-            const int* rl34 = A.r34.len[L4][L3];
-            if (!rl34) continue;
-            int len34 = rl34[i4];
-            if (!len34) continue;
-            float b34 = A.pb34[A.r34.start[L4][L3][i4]];
-            if (b34 < thre34) continue;
-            if ((double) (b12 * b34) * dmax < (double) A.thresp) continue;
-            int c = combo_index(L1, L2, L3, L4);
-            int slot = atomicAdd(&A.ntask[c], 1);
-            A.tasks[A.cap_off[c] + slot] = KTask{i2, i4, dmax};
-            if (A.split && (double) (b12 * b34) * dmax >= (double) A.thredp) {
-                int hs = atomicAdd(&A.ntask_hi[c], 1);
-                A.tasks_hi[A.cap_off[c] + hs] = KTask{i2, i4, dmax};
+            bool want = false;
+            float b34 = 0.0f;
+            if (valid) {
+                const int* rl34 = A.r34.len[L4][L3];
+                if (rl34 && rl34[i4]) {
+                    b34 = A.pb34[A.r34.start[L4][L3][i4]];
+                    want = b34 >= thre34 && (double) (b12 * b34) * dmax >= (double) A.thresp;
+                }
             }
+            const int c = combo_index(L1, L2, L3, L4);
+            const KTask t{i2, i4, dmax};
+            const unsigned wm = __ballot_sync(0xffffffffu, want);
+            if (want) append_task(wm, c, A.cap_off[c], A.ntask, A.tasks, t);
+            const bool hi = want && A.split && (double) (b12 * b34) * dmax >= (double) A.thredp;
+            const unsigned hm = __ballot_sync(0xffffffffu, hi);
+            if (hi) append_task(hm, c, A.cap_off[c], A.ntask_hi, A.tasks_hi, t);
         }
     }
 }
-
-
 
 // Runtime (L1,L2,L3,L4) -> template dispatch.
 template <int L1, int L2, int L3>
