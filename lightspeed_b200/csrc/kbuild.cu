@@ -116,8 +116,8 @@ __device__ __forceinline__ void append_task(unsigned want_mask, int c, long off,
 
 __global__ void k_task_gen(TaskGenArgs A)
 {
-    const int i2 = blockIdx.y;
-    const int i4 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i2 = blockIdx.x;
+    const int i4 = blockIdx.y * blockDim.x + threadIdx.x;
     // exchange.cpp:137-139 (prim2 <= prim4 for a symmetric D24); lanes out of
     // range stay for the warp-wide votes below
     const bool valid = i4 < A.b4.nprim && !(A.d24symm && i2 > i4);
@@ -283,7 +283,9 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     G.thredp = thredp;
     G.split = mixed ? 1 : 0;
     if (b2->nprim && b4->nprim && pl12->kdat.nent && pl34->kdat.nent) {
-        dim3 grid(nblk(b4->nprim, 128), b2->nprim);
+        // prim2 varies fastest over the blocks, so the lists interleave prim2 rows: warps taking
+        // neighbouring tasks then mostly add into different K13 rows
+        dim3 grid(b2->nprim, nblk(b4->nprim, 128));
         k_task_gen<<<grid, 128, 0, s>>>(G);
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches++;
