@@ -198,7 +198,8 @@ int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const double* scal
  * are formed on the device and go through the batched J path 16 at a time;
  * J never leaves the device. The flags stand for the reference's
  * pointer-identity tests and select its symmetrisations (mo_eri.cpp:121-155):
- * sym12 for C1 == C2, sym34 for C3 == C4, sym1234 for C1 == C3 and C2 == C4. */
+ * sym12 for C1 == C2, sym34 for C3 == C4, sym1234 for C1 == C3 and C2 == C4.
+ * n3 is at most 65535 (LSJK_EINVAL above). */
 int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
                const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int n1, int n2, int n3, int n4,
                const double* C1, const double* C2, const double* C3, const double* C4, int sym12, int sym34,

@@ -865,6 +865,7 @@ extern "C" int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, co
         if (n1 < 0 || n2 < 0 || n3 < 0 || n4 < 0) throw lsjk::Error(LSJK_EINVAL, "negative orbital count");
         if ((sym12 && n1 != n2) || (sym34 && n3 != n4) || (sym1234 && (n1 != n3 || n2 != n4)))
             throw lsjk::Error(LSJK_EINVAL, "a symmetry flag needs equal orbital counts");
+        if (n3 > 65535) throw lsjk::Error(LSJK_EINVAL, "lsjk_eri_j: at most 65535 orbitals in C3");
         const size_t nI = (size_t) n1 * n2 * n3 * n4;
         if (nI && (!C1 || !C2 || !C3 || !C4 || !I)) throw lsjk::Error(LSJK_EINVAL, "null argument");
         lsjk::Context* c = &ctx->c;
