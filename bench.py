@@ -60,6 +60,7 @@ def parse():
 
 
 def dist_info():
+    # read here (not through lightspeed_b200.replicas) so the reference arm never loads the engine
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -197,10 +198,8 @@ def run_ours(args):
     import torch
     torch.cuda.set_device(local)
     os.environ.setdefault("LSJK_DEVICE", str(local))
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from lightspeed_b200 import replicas
+    replicas.init("nccl", timeout_s=600)
     import lightspeed_b200 as ls
     from lightspeed_b200.scf import RHF
     mol, bas = workload(ls, args.carbons)
@@ -286,9 +285,7 @@ def run_ours(args):
     # ---- timed region -------------------------------------------------------
     clocks = Clocks(local)
     clocks.start()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     launches0 = ls.stats()["kernel_launches"]
     ms64, msk64 = timed(ls.PREC_FP64, THREDP, args.steps)
@@ -312,31 +309,20 @@ def run_ours(args):
         s1.record(stream)
         s1.synchronize()
         e2e_ms += max(s0.elapsed_time(s1), 1e3 * (time.time() - t_host))
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
 
-    def agg(x):
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([x], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
-
-    ms64, msk64, msmx, mskmx, e2e_ms = (agg(v) for v in (ms64, msk64, msmx, mskmx, e2e_ms))
+    # every timing as its maximum over the ranks (one all-reduce)
+    ms64, msk64, msmx, mskmx, e2e_ms = replicas.max_over_ranks([ms64, msk64, msmx, mskmx, e2e_ms], device=dev)
     if rank != 0:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        replicas.finish()
         return 0
     q64 = counts["fp64"]["j_quartets"] + counts["fp64"]["k_quartets"]
     qmx = counts["mixed"]["j_quartets"] + counts["mixed"]["k_quartets"]
-    fp64_qps = world * q64 * args.steps / (ms64 * 1e-3)
-    mixed_qps = world * qmx * args.steps / (msmx * 1e-3)
-    e2e_qps = world * qmx * args.steps / (e2e_ms * 1e-3)
+    fp64_qps = replicas.whole_job_rate(q64 * args.steps, world, ms64 * 1e-3)
+    mixed_qps = replicas.whole_job_rate(qmx * args.steps, world, msmx * 1e-3)
+    e2e_qps = replicas.whole_job_rate(qmx * args.steps, world, e2e_ms * 1e-3)
     peak64 = ls.fma_peak_tflops(True)
     peak32 = ls.fma_peak_tflops(False)
     # roofline of the dominant kernel family (the K kernels, FP64 path)
@@ -393,9 +379,7 @@ def run_ours(args):
         "cpu_baseline": cpu,
     }
     print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish()
     return 0
 
 
