@@ -80,8 +80,9 @@ class Clocks:
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                                 ".clocks_%d.csv" % os.getpid())
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="lsjk_clocks_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"

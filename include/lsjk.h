@@ -5,7 +5,7 @@
  * closed TeraChem library behind IntBox::coulombTC / exchangeTC
  * (src/cpp/intbox/tc/coulomb.cpp:14-63, tc/exchange.cpp:14-77 in the reference)
  * and is called from the C++ IntBox::coulomb / IntBox::exchange shim in
- * lightspeed_b200/csrc/host/intbox.cpp, which keeps the reference signatures
+ * lightspeed_b200/csrc/host/lightspeed.cpp, which keeps the reference signatures
  * (src/lightspeed/intbox.hpp:761-771 and :817-828).
  *
  * Conventions

@@ -48,16 +48,23 @@ __device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, d
     }
 }
 
+// Start of the last bin of the Boys table: from here on (the bin next to the
+// switch to the asymptotic form, and the asymptotic region itself) the FP32
+// path evaluates the Boys function in FP64 by its asymptotic form.
+constexpr float kBoysSwitch32 = (float) (LSJK_BOYS_TMAX - LSJK_BOYS_TMAX / LSJK_BOYS_NBIN);
+
 // The same quartet in FP32 (geometry differences formed in FP64, everything
-// else in FP32), added to the FP64 accumulators.
+// else in FP32 except the Boys function at T >= kBoysSwitch32, which is
+// evaluated in FP64 by its asymptotic form), added to the FP64 accumulators.
 template <int LB, int LK, int NG>
-__device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, float p, double Px, double Py,
-                                            double Pz, const double* __restrict__ r, const float* __restrict__ r32,
-                                            double (*jp)[nherm_of(LB)])
+__device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, float p,
+                                            double Px, double Py, double Pz, const double* __restrict__ r,
+                                            const float* __restrict__ r32, double (*jp)[nherm_of(LB)])
 {
     constexpr int L = LB + LK, HB = nherm_of(LB), HK = nherm_of(LK);
     const float q = r32[0];
-    const float X = (float) (Px - r[1]), Y = (float) (Py - r[2]), Z = (float) (Pz - r[3]);
+    const double Xd = Px - r[1], Yd = Py - r[2], Zd = Pz - r[3];
+    const float X = (float) Xd, Y = (float) Yd, Z = (float) Zd;
     const float R2 = X * X + Y * Y + Z * Z;
     const float rs = rsqrtf(p + q);
     const float rho = p * q * (rs * rs);
@@ -76,7 +83,12 @@ __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, fl
         }
         const float rhoe = rho * d2;
         float F[L + 1];
-        boys_eval<L, float>(rhoe * R2, tab, F);
+        const float T = rhoe * R2;
+        if (T < kBoysSwitch32) {
+            boys_eval<L, float>(T, tab, F);
+        } else {
+            boys_asym_f64_to_f32<L>((double) rhoe * (Xd * Xd + Yd * Yd + Zd * Zd), F);
+        }
         float a[L + 1];
         const float m2r = -2.0f * rhoe;
         float pw = f;

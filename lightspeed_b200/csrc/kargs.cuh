@@ -56,6 +56,11 @@ struct KArgs {
     const void* rys;          // table block of this rule, in the pass precision
     const void* asym_t;
     const void* asym_w;
+    // FP64 table block and asymptotic nodes of this rule in global memory: the
+    // FP32 pass evaluates the roots and weights in FP64 from the last table bin on
+    const double* rys64g;
+    const double* asym64_t;
+    const double* asym64_w;
     int nbin;
     double tmax;
     int* status;

@@ -360,6 +360,9 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.rys = ctx->rys64.p + kRysOffset[NR];
                     A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
                     A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                    A.rys64g = ctx->rys64.p + kRysOffset[NR];
+                    A.asym64_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
+                    A.asym64_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
                     A.qcount = qcnt + c;
                     auto tune = [&](const KArgs& X, bool fp32) {
                         // autotuner: time candidate grid sizes on scratch outputs

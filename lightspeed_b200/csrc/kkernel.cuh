@@ -148,7 +148,26 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
             f *= sqrt(d2);
         }
         R t2[NR], w[NR];
-        rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
+        if constexpr (sizeof(R) == 4) {
+            // FP32 pass: from the last table bin on (the bin next to the switch to the
+            // asymptotic form, and the asymptotic region) the roots and weights are the
+            // FP64 asymptotic form t = s / sqrt(T), w = h / sqrt(T), which over the last
+            // bin already agrees with the exact rule to ~1e-13 relative
+            const R T = rho * d2 * RR;
+            if (T < tmax - tmax / (R) A.nbin) {
+                rys_eval<NR, R>(T, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
+            } else {
+                const double r = rsqrt((double) rho * (double) d2 * (double) RR);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const double t = A.asym64_t[i] * r;
+                    t2[i] = (R) (t * t);
+                    w[i] = (R) (A.asym64_w[i] * r);
+                }
+            }
+        } else {
+            rys_eval<NR, R>(rho * d2 * RR, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
+        }
         auto root = [&](int r) {
             const R u = t2[r] * d2 * ipq;
             const R qu = q * u, pu = p * u;

@@ -195,6 +195,27 @@ __device__ __forceinline__ void rys_eval(R T, const R* __restrict__ tab, int nbi
     }
 }
 
+// Boys values F_0..F_L at T >= LSJK_BOYS_TMAX - (one bin) by the FP64
+// asymptotic form F_0 = sqrt(pi/T)/2 and the upward recursion with the exp(-T)
+// term, rounded to FP32 (the FP32 J path from the last table bin on: over that
+// bin the form already agrees with the exact function to ~1e-16 relative).
+template <int L>
+__device__ __forceinline__ void boys_asym_f64_to_f32(double T, float* __restrict__ F)
+{
+    const double r = rsqrt(T);
+    double f = 0.88622692545275801364908374167057259 * r;   // sqrt(pi)/2 / sqrt(T)
+    F[0] = (float) f;
+    if (L > 0) {
+        const double e = exp(-T);
+        const double h = 0.5 * r * r;
+#pragma unroll
+        for (int m = 0; m < L; ++m) {
+            f = (double(2 * m + 1) * f - e) * h;
+            F[m + 1] = (float) f;
+        }
+    }
+}
+
 // Cartesian component count of a shell and Hermite count of a pair.
 __host__ __device__ constexpr int ncart_of(int L) { return (L + 1) * (L + 2) / 2; }
 __host__ __device__ constexpr int nherm_of(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }

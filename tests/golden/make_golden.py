@@ -10,7 +10,7 @@ reference tree and oracle/_ref built; the fixtures are committed).
    D = C C^T of 40 seeded Gaussian columns Loewdin-orthonormalised in the
    reference overlap metric; plus the pair list of that basis.
 
-  python tests/golden/make_golden.py /root/reference
+  python tests/golden/make_golden.py [REFERENCE_ROOT]   (default: $REFROOT, else /root/reference)
 """
 import os
 import sys
@@ -66,7 +66,7 @@ def oracle_water8():
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFROOT", "/root/reference")
     copy_reference_vectors(ref_root)
     oracle_water8()
     print("golden fixtures written to", HERE)

@@ -1,0 +1,160 @@
+"""Parity at the sizes of the benchmark workloads, against the oracle (the
+reference CPU IntBox built from its sources, oracle/_ref).
+
+* C40H82 / cc-pVDZ (970 functions, 1290 primitive shells), Schwarz 1e-14, at
+  the converged RHF density: J in FP64 elementwise within 1e-10 of the
+  reference coulombCPU, and mixed-precision J (thredp = 1e-5) within 1e-6.
+  (The reference's K for this system takes tens of CPU minutes, so K is
+  checked on the shorter alkane below, whose quartets are the same kinds.)
+* C10H22 / cc-pVDZ at its converged density: J and symmetric K in FP64 within
+  1e-10 of coulombCPU / exchangeCPU, and the mixed-precision build at the
+  workload's thredp = 1e-5 within 1e-6 elementwise and |dE| <= 1e-6 Eh at fixed
+  density.
+* A mixed-precision RHF of C10H22 (incremental Fock, thredp = 1e-5) converges
+  to the FP64 RHF energy within 1e-6 Eh.
+* Batched K: four non-symmetric densities in one exchangeMulti call, bare
+  Coulomb and erf-attenuated (omega = 0.3) operators, each against the
+  reference exchangeCPU of that density within 1e-10.
+"""
+import numpy as np
+import pytest
+
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+THRE = 1.0e-14
+THREDP = 1.0e-5
+
+
+def _need_ref():
+    if not ref.available():
+        pytest.skip("oracle/_ref (reference CPU IntBox) not built")
+
+
+def _alkane_scf(ls, ncarbon):
+    from lightspeed_b200.geometry import alkane
+    from lightspeed_b200.sad import SAD
+    from lightspeed_b200.scf import RHF
+    mol = alkane(ncarbon)
+    bas = ls.Basis.from_gbs_file(mol, "cc-pvdz")
+    ls.set_precision(ls.PREC_FP64)
+    scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
+    E = scf.compute(D0=SAD(ls, "cc-pvdz").density(mol, bas), maxiter=60, g_conv=1e-6)
+    assert scf.converged
+    return mol, bas, scf, E
+
+
+def _ref_pairs(bas):
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    return ref.RefPairs(rb, rb, True, THRE)
+
+
+def _builds(ls, scf, D, thredp):
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    Dt = ls.Tensor.array(D)
+    J = ls.IntBox.coulomb(res, ew, scf.pairs, scf.pairs, Dt, THRE, thredp).np.copy()
+    K = ls.IntBox.exchange(res, ew, scf.pairs, scf.pairs, Dt, True, THRE, thredp).np.copy()
+    return J, K
+
+
+@pytest.fixture(scope="module")
+def c10(ls):
+    _need_ref()
+    try:
+        mol, bas, scf, E = _alkane_scf(ls, 10)
+        rp = _ref_pairs(bas)
+        D = scf.D.copy()
+        Jr = ref.coulomb(rp, rp, D, THRE, THRE)
+        Kr = ref.exchange(rp, rp, D, True, THRE, THRE)
+        yield {"scf": scf, "E": E, "D": D, "Jr": Jr, "Kr": Kr}
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
+
+
+def test_c10h22_fp64_vs_oracle(ls, c10):
+    ls.set_precision(ls.PREC_FP64)
+    J, K = _builds(ls, c10["scf"], c10["D"], THRE)
+    assert np.max(np.abs(J - c10["Jr"])) < 1e-10
+    assert np.max(np.abs(K - c10["Kr"])) < 1e-10
+
+
+def test_c10h22_mixed_vs_oracle(ls, c10):
+    ls.set_precision(ls.PREC_MIXED)
+    ls.reset_stats()
+    J, K = _builds(ls, c10["scf"], c10["D"], THREDP)
+    st = ls.stats()
+    assert st["quartets_fp32"] > st["quartets_fp64"]
+    D = c10["D"]
+    assert np.max(np.abs(J - c10["Jr"])) < 1e-6
+    assert np.max(np.abs(K - c10["Kr"])) < 1e-6
+    dE = float(np.sum(D * (2.0 * (J - c10["Jr"]) - (K - c10["Kr"]))))
+    assert abs(dE) < 1e-6
+
+
+def test_c10h22_mixed_scf_energy(ls, c10):
+    """Mixed-precision RHF (the workload's thredp) against the FP64 RHF."""
+    from lightspeed_b200.sad import SAD
+    from lightspeed_b200.scf import RHF
+    scf64 = c10["scf"]
+    ls.set_precision(ls.PREC_MIXED)
+    scf = RHF(ls, scf64.mol, scf64.basis, thre_pq=THRE, thre_sp=THRE, thre_dp=THREDP)
+    E = scf.compute(D0=SAD(ls, "cc-pvdz").density(scf64.mol, scf64.basis), maxiter=60, g_conv=1e-6)
+    assert scf.converged
+    assert abs(E - c10["E"]) < 1e-6
+
+
+@pytest.fixture(scope="module")
+def c40(ls):
+    _need_ref()
+    try:
+        mol, bas, scf, E = _alkane_scf(ls, 40)
+        assert bas.nao == 970 and bas.nprim == 1290
+        D = scf.D.copy()
+        rp = _ref_pairs(bas)
+        Jr = ref.coulomb(rp, rp, D, THRE, THRE)
+        yield {"scf": scf, "D": D, "Jr": Jr}
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
+
+
+def test_c40h82_j_vs_oracle(ls, c40):
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    pl = c40["scf"].pairs
+    Dt = ls.Tensor.array(c40["D"])
+    ls.set_precision(ls.PREC_FP64)
+    J = ls.IntBox.coulomb(res, ew, pl, pl, Dt, THRE, THRE).np.copy()
+    assert np.max(np.abs(J - c40["Jr"])) < 1e-10
+    ls.set_precision(ls.PREC_MIXED)
+    Jm = ls.IntBox.coulomb(res, ew, pl, pl, Dt, THRE, THREDP).np.copy()
+    assert np.max(np.abs(Jm - c40["Jr"])) < 1e-6
+    assert abs(2.0 * float(np.sum(c40["D"] * (Jm - c40["Jr"])))) < 1e-6
+
+
+@pytest.mark.parametrize("ewald", [([1.0], [-1.0]), ([1.0], [0.3])])
+def test_batched_k_vs_oracle(ls, ewald):
+    """exchangeMulti of four non-symmetric rank-3 densities (one shared task
+    list and quartet loop) against one reference exchangeCPU per density."""
+    _need_ref()
+    from lightspeed_b200.geometry import water_cluster
+    ls.set_precision(ls.PREC_FP64)
+    try:
+        bas = ls.Basis.from_gbs_file(water_cluster(4, seed=3), "6-31gs")
+        pl = ls.PairList.build_schwarz(bas, bas, True, THRE)
+        rng = np.random.default_rng(17)
+        Dn = []
+        for _ in range(4):
+            X = rng.standard_normal((bas.nao, 3)) / np.sqrt(bas.nao)
+            Y = rng.standard_normal((bas.nao, 3)) / np.sqrt(bas.nao)
+            Dn.append(X @ Y.T)
+        res = ls.ResourceList.build()
+        ew = ls.Ewald(*ewald)
+        Km = ls.IntBox.exchangeMulti(res, ew, pl, pl, [ls.Tensor.array(D) for D in Dn], False, THRE, THRE)
+        rp = _ref_pairs(bas)
+        for D, K in zip(Dn, Km):
+            Kr = ref.exchange(rp, rp, D, False, THRE, THRE, *ewald)
+            assert np.max(np.abs(K.np - Kr)) < 1e-10
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
