@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--carbons", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-merge", action="store_true",
+                    help="alkane: K over the primitives as given (the reference's exact quartet set) instead of "
+                         "the merged twins")
     ap.add_argument("--scf-maxiter", type=int, default=60)
     ap.add_argument("--workload", default="alkane", choices=["alkane", "batched", "guess", "many", "eri"],
                     help="alkane: the headline C40H82 J+K step; batched: 64 response-like densities "
@@ -121,29 +124,38 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_sample():
-    """Bounded CPU sample of the workload: C8H18 / cc-pVDZ (all-trans, same
-    thresholds) with its core-Hamiltonian density, built from the reference
-    CPU IntBox alone (S, T, V) so the reference arm runs no code of ours;
-    quartets are counted by the oracle's shared counting routine."""
-    import lightspeed_b200 as ls
-    from oracle import port, ref
-    mol, bas = workload(ls, SAMPLE_CARBONS)
-    rb = ref.RefBasis(ref.prim_arrays(bas))
+    """Bounded CPU sample of the workload: C8H18 / cc-pVDZ (all-trans, the same
+    basis, thresholds and operator), full J + K at its converged RHF density
+    (tests/golden/c8h18_ccpvdz_cocc.npz, converged by the reference CPU
+    IntBox itself). Geometry, basis and density come from oracle/ alone, so
+    this path loads no code of the product; quartets are counted by the
+    oracle's counting routine (the reference quartet set)."""
+    from oracle import port, ref, workloads
+    symbols, xyz = workloads.alkane(SAMPLE_CARBONS)
+    arrays, prims, nao = workloads.basis(symbols, xyz, "cc-pvdz")
+    rb = ref.RefBasis(arrays)
     rp = ref.RefPairs(rb, rb, True, THRE)
-    S = ref.overlap(rp)
-    H = ref.kinetic(rp) + ref.potential(rp, mol.xyzZ)
-    s, U = np.linalg.eigh(S)
-    X = U / np.sqrt(s)
-    e, C = np.linalg.eigh(X.T @ H @ X)
-    nocc = int(round(mol.nuclear_charge)) // 2
-    Cocc = (X @ C)[:, :nocc]
-    D = Cocc @ Cocc.T
-    pb = port.Basis(bas.primitives)
+    z = np.load(os.path.join(ROOT, "tests", "golden", "c%dh%d_ccpvdz_cocc.npz" % (SAMPLE_CARBONS,
+                                                                                2 * SAMPLE_CARBONS + 2)))
+    C = z["Cocc"]
+    D = C @ C.T
+    pb = port.Basis(prims)
     ppl = port.Pairs(pb, pb, True, THRE)
     nj, nk = port.count_quartets(ppl, ppl, D, D, True, THRE)
-    desc = ("C%dH%d/cc-pVDZ (%d bf) full J+K, FP64, thresp 1e-14, core-Hamiltonian density; "
-            "%.4g quartets per J+K" % (SAMPLE_CARBONS, 2 * SAMPLE_CARBONS + 2, bas.nao, nj + nk))
+    desc = ("C%dH%d/cc-pVDZ (%d bf) full J+K, FP64, thre_pq = thresp = 1e-14, at its converged RHF density "
+            "(reference CPU IntBox SCF); %.4g quartets per J+K (J %.4g, K %.4g)" % (
+                SAMPLE_CARBONS, 2 * SAMPLE_CARBONS + 2, nao, nj + nk, nj, nk))
     return rp, D, nj + nk, desc
 
 
@@ -161,9 +173,17 @@ def cpu_baseline(nthread):
     if not (ref.available() and port.available()):
         return {"error": "oracle/_ref not built"}
     rp, D, nq, desc = cpu_sample()
+    time_reference(rp, D, nthread)   # warm-up (J and K)
     dt = time_reference(rp, D, nthread)
-    return {"value": nq / dt, "unit": "quartets/s", "cores": nthread, "kind": "reference",
+    return {"value": nq / dt, "unit": "quartets/s", "cores": nthread, "cpu_model": cpu_model(), "kind": "reference",
             "sample": desc + "; %.2f s" % dt, "seconds": dt}
+
+
+def workload_config(ncarbon):
+    """The workload as both arms name it."""
+    return {"workload": "C%dH%d/cc-pVDZ full J+K build at the converged RHF density" % (ncarbon, 2 * ncarbon + 2),
+            "thre_pq": THRE, "thresp": THRE, "thredp": THREDP, "operator": "1/r",
+            "l2": "flushed between steps (256 MiB write outside the timed events)"}
 
 
 def run_reference(args):
@@ -176,9 +196,8 @@ def run_reference(args):
         return 0
     nthread = os.cpu_count() or 1
     rp, D, nq, desc = cpu_sample()
-    from oracle import ref as _r
     for _ in range(args.warmup):
-        _r.coulomb(rp, rp, D, THRE, THRE, nthread=nthread)
+        time_reference(rp, D, nthread)
     times = [time_reference(rp, D, nthread) for _ in range(args.steps)]
     T = float(np.sum(times))
     v = nq * args.steps / T
@@ -186,9 +205,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "quartets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "C40H82/cc-pVDZ J+K, timed on a bounded sample", "sample": desc},
-        "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": nthread, "kind": "reference",
-                         "sample": desc},
+        "config": workload_config(args.carbons),
+        "cpu_baseline": {"value": v, "unit": "quartets/s", "cores": nthread, "cpu_model": cpu_model(),
+                         "kind": "reference", "sample": desc},
         "e2e": {"value": v, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
     return 0
@@ -246,11 +265,18 @@ def run_ours(args):
             ms_k += e1.elapsed_time(e2)
         return ms_total, ms_k
 
-    # warm-up in both modes
-    for mode in (ls.PREC_FP64, ls.PREC_MIXED):
-        ls.set_precision(mode)
-        for _ in range(args.warmup):
-            step(THREDP)
+    # the headline runs K over the merged twins (shared s exponents computed once);
+    # the exact reference quartet set (merging off) is timed beside it
+    merge = not args.no_merge
+    ls.set_merge(merge)
+    # warm-up in both precision modes (and in exact mode, timed below too)
+    for mg in ((merge, False) if merge else (False,)):
+        ls.set_merge(mg)
+        for mode in (ls.PREC_FP64, ls.PREC_MIXED):
+            ls.set_precision(mode)
+            for _ in range(args.warmup):
+                step(THREDP)
+    ls.set_merge(merge)
     torch.cuda.synchronize()
     if args.profile_step:
         ls.set_precision(ls.PREC_FP64)
@@ -265,7 +291,7 @@ def run_ours(args):
         torch.cuda.profiler.stop()
         print(json.dumps({"profile_step": True, "workload": "C%dH%d/cc-pVDZ" % (args.carbons, 2 * args.carbons + 2)}))
         return 0
-    # quartet/flop counts of one step in each mode
+    # quartet/flop counts of one step in each mode (the quartets the merged build computes)
     counts = {}
     for name, mode in (("fp64", ls.PREC_FP64), ("mixed", ls.PREC_MIXED)):
         ls.set_precision(mode)
@@ -274,14 +300,29 @@ def run_ours(args):
         torch.cuda.synchronize()
         counts[name] = dict(ls.stats())
         counts[name].update({"flops_" + k: v for k, v in ls.flops_split().items()})
-    # energies at the converged density: E(D) with FP64 vs mixed J/K
+    # the workload's quartets in the reference's definition: the same step over the
+    # primitives as given (merging off), whose counters equal the reference quartet set
+    ls.set_merge(False)
+    ls.set_precision(ls.PREC_FP64)
+    ls.reset_stats()
+    step(THREDP)
+    torch.cuda.synchronize()
+    st_ref = ls.stats()
+    q_ref = st_ref["j_quartets"] + st_ref["k_quartets"]
+    ls.set_merge(merge)
+    # energies at the converged density: E(D) with FP64 vs mixed J/K, and the
+    # headline's FP64 build against the exact reference quartet set
     energies = {}
-    for name, mode in (("fp64", ls.PREC_FP64), ("mixed", ls.PREC_MIXED)):
+    for name, mode, mg in (("fp64", ls.PREC_FP64, merge), ("mixed", ls.PREC_MIXED, merge),
+                           ("fp64_exact", ls.PREC_FP64, False)):
+        ls.set_merge(mg)
         ls.set_precision(mode)
         J = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), THRE, THREDP).np
         K = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, THRE, THREDP).np
         energies[name] = scf.energy(D, J, K)[0]
+    ls.set_merge(merge)
     dE = energies["mixed"] - energies["fp64"]
+    dE_merge = energies["fp64"] - energies["fp64_exact"]
 
     # ---- timed region -------------------------------------------------------
     clocks = Clocks(local)
@@ -294,6 +335,14 @@ def run_ours(args):
     msmx, mskmx = timed(ls.PREC_MIXED, THREDP, args.steps)
     torch.cuda.synchronize()
     launches_timed = ls.stats()["kernel_launches"] - launches0
+    exact = {}
+    if merge:
+        ls.set_merge(False)
+        ex64, exk64 = timed(ls.PREC_FP64, THREDP, args.steps)
+        exmx, exkmx = timed(ls.PREC_MIXED, THREDP, args.steps)
+        ls.set_merge(True)
+        exact = {"fp64_ms": ex64 / args.steps, "fp64_ms_k": exk64 / args.steps, "mixed_ms": exmx / args.steps,
+                 "mixed_ms_k": exkmx / args.steps}
     # e2e through the public host API (each call copies D host->device; J and K come back)
     Dt = ls.Tensor.array(D)
     e2e_ms = 0.0
@@ -319,11 +368,12 @@ def run_ours(args):
     if rank != 0:
         replicas.finish()
         return 0
+    # computed quartets (merged twins) and the workload's reference quartet count
     q64 = counts["fp64"]["j_quartets"] + counts["fp64"]["k_quartets"]
     qmx = counts["mixed"]["j_quartets"] + counts["mixed"]["k_quartets"]
-    fp64_qps = replicas.whole_job_rate(q64 * args.steps, world, ms64 * 1e-3)
-    mixed_qps = replicas.whole_job_rate(qmx * args.steps, world, msmx * 1e-3)
-    e2e_qps = replicas.whole_job_rate(qmx * args.steps, world, e2e_ms * 1e-3)
+    fp64_qps = replicas.whole_job_rate(q_ref * args.steps, world, ms64 * 1e-3)
+    mixed_qps = replicas.whole_job_rate(q_ref * args.steps, world, msmx * 1e-3)
+    e2e_qps = replicas.whole_job_rate(q_ref * args.steps, world, e2e_ms * 1e-3)
     peak64 = ls.fma_peak_tflops(True)
     peak32 = ls.fma_peak_tflops(False)
     # roofline of the dominant kernel family (the K kernels, FP64 path)
@@ -348,16 +398,24 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64+f32 (mixed)",
         "data": "synthetic",
-        "config": {"workload": "C%dH%d/cc-pVDZ full J+K build at the converged RHF density" % (
-            args.carbons, 2 * args.carbons + 2), "nao": nao, "ncart": bas.ncart, "nprim": bas.nprim,
-            "thre_pq": THRE, "thresp": THRE, "thredp": THREDP, "operator": "1/r",
-            "l2": "flushed between steps (256 MiB write outside the timed events)",
-            "parallelism": "replicas" if world > 1 else "single-gpu", "scf_iterations": len(scf.trace),
-            "scf_energy": E_scf, "scf_converged": bool(scf.converged), "scf_guess": "SAD", "scf_seconds": t_scf},
+        "config": workload_config(args.carbons),
+        "system": {"nao": nao, "ncart": bas.ncart, "nprim": bas.nprim,
+                   "parallelism": "replicas" if world > 1 else "single-gpu", "scf_iterations": len(scf.trace),
+                   "scf_energy": E_scf, "scf_converged": bool(scf.converged), "scf_guess": "SAD",
+                   "scf_seconds": t_scf},
+        # K over merged twins (shared s exponents computed once; ls.set_merge): the same K up to
+        # quartets below thresp (dE_merged_vs_exact_Eh at fixed density); "exact" is the same
+        # step over the reference's exact quartet set
+        "merged_s_exponents": merge, "dE_merged_vs_exact_Eh": dE_merge if merge else 0.0, "exact": exact,
+        # quartets: the reference's quartet set of the step (its J and K screens over the
+        # primitives as given); quartets_computed: what the merged build evaluates
+        "quartets": q_ref, "quartets_ref_j": st_ref["j_quartets"], "quartets_ref_k": st_ref["k_quartets"],
         "fp64": {"ms_per_iter": ms64 / args.steps, "quartets_per_s": fp64_qps, "ms_k": msk64 / args.steps,
-                 "quartets": q64, "gpu_launches_per_step": launches_fp64 / max(args.steps, 1)},
+                 "quartets_computed": q64, "computed_per_s": q64 / (ms64 / args.steps * 1e-3),
+                 "gpu_launches_per_step": launches_fp64 / max(args.steps, 1)},
         "mixed": {"ms_per_iter": msmx / args.steps, "quartets_per_s": mixed_qps, "ms_k": mskmx / args.steps,
-                  "quartets_fp32": counts["mixed"]["quartets_fp32"], "quartets": qmx,
+                  "quartets_fp32": counts["mixed"]["quartets_fp32"], "quartets_computed": qmx,
+                  "computed_per_s": qmx / (msmx / args.steps * 1e-3),
                   "speedup_vs_fp64": ms64 / msmx, "dE_vs_fp64_Eh": dE},
         "roofline": {"bound": "fp64", "kernel": "k_exchange (K build, FP64)", "achieved": achieved,
                      "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,

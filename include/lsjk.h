@@ -74,6 +74,21 @@ const char* lsjk_version(void);
 int lsjk_context_create(int device, lsjk_context** out);
 int lsjk_context_destroy(lsjk_context* ctx);
 int lsjk_context_set_precision(lsjk_context* ctx, int mode);
+/* Merge mode for K (on = 1; off, the default). Some basis sets (cc-pVXZ, ANO)
+ * repeat one s exponent of an atom in several contracted shells; the
+ * reference treats every copy as a primitive of its own
+ * (src/cpp/core/pair_list.cpp:29-177). In merge mode each basis carries a
+ * twin with one primitive per distinct (atom, s exponent); K builds compute
+ * each of its integrals once and contract it into every shell that shares
+ * it, screening with bounds that cover every copy, so every quartet the
+ * reference keeps is kept (plus copies just below thresp): K equals the
+ * reference's within the size of those sub-threshold quartets (~1e-11 on
+ * C10H22-C40H82 / cc-pVDZ at thresp 1e-14, ~2e-12 on a small molecule), with
+ * fewer quartets computed. Off: K runs over the primitives as given, the
+ * reference's exact quartet set (the counters then equal the reference's
+ * count). J always runs over the primitives as given. No counterpart in the
+ * reference. */
+int lsjk_context_set_merge(lsjk_context* ctx, int on);
 /* The CUDA stream (cudaStream_t) the context enqueues on, as void*. */
 void* lsjk_context_stream(lsjk_context* ctx);
 int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out);

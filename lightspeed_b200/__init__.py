@@ -13,7 +13,7 @@ from ._lightspeed import (Tensor, Primitive, Basis, Pair, PairListL, PairList, E
                           PREC_MIXED, PREC_FP64, set_precision, get_precision, stats, reset_stats,
                           engine_version, stream_handle, fma_peak_tflops, coulomb_device, exchange_device,
                           graph_begin, graph_end, Graph, class_counts, Stream, flops_split,
-                          set_autotune, get_tune_table, set_tune_table)
+                          set_autotune, get_tune_table, set_tune_table, set_merge, get_merge)
 from .molecule import Atom, Molecule, units
 from . import gbs as _gbs
 
@@ -44,4 +44,4 @@ Basis.basisdir = _gbs.BASIS_DIR
 
 __all__ = ["Tensor", "Primitive", "Basis", "Pair", "PairListL", "PairList", "Ewald", "ResourceList", "IntBox",
            "Atom", "Molecule", "units", "PREC_MIXED", "PREC_FP64", "set_precision", "get_precision", "stats",
-           "reset_stats", "engine_version", "LIB_PATH"]
+           "reset_stats", "engine_version", "set_merge", "get_merge", "LIB_PATH"]

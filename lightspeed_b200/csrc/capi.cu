@@ -108,6 +108,33 @@ void check_lmax(const lsjk::PairList* pl)
         throw lsjk::Error(LSJK_ENOTSUPP, "J/K: angular momentum above d is not supported by the GPU kernels");
 }
 
+// The pair list a K build runs over: its merged twin (shared s exponents of a
+// basis computed once) unless the context builds over the primitives as given.
+// J builds always run over the primitives as given: merging their screens
+// moves J by up to ~1e-10 on the largest workload, while merged K stays within
+// ~2e-11 of the reference's quartet set.
+const lsjk::PairList* effective(const lsjk::Context* ctx, const lsjk::PairList* pl)
+{
+    return (ctx->merge && pl->twin) ? pl->twin.get() : pl;
+}
+
+// Screening densities for a K build over twins (u3 x u4, standing for the
+// caller's bases o3 x o4): the density in the caller's Cartesian layout,
+// then per twin slot the largest weighted |D| of its copies. Null when
+// neither side is a twin (the screens then read the density itself).
+void screening_densities(lsjk::Context* ctx, const lsjk::Basis* o3, const lsjk::Basis* o4, const lsjk::Basis* u3,
+                         const lsjk::Basis* u4, const double* const* Dpure, int ng, double** Dscr)
+{
+    for (int g = 0; g < ng; ++g) Dscr[g] = nullptr;
+    if (u3 == o3 && u4 == o4) return;
+    double* Dorig = lsjk::take<double>(ctx, (size_t) o3->ncart * o4->ncart);
+    for (int g = 0; g < ng; ++g) {
+        Dscr[g] = lsjk::take<double>(ctx, (size_t) u3->ncart * u4->ncart);
+        lsjk::pure_to_cart(ctx, o3, o4, Dpure[g], Dorig);
+        lsjk::screen_density(ctx, u3, u4, Dorig, o4->ncart, Dscr[g]);
+    }
+}
+
 // One J build for ng (1..4) densities that share the quartet loop, device
 // pointers in and out.
 void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
@@ -130,13 +157,17 @@ void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairLi
 }
 
 // One K build for ng (1..4) densities sharing the quartet integrals, device
-// pointers in and out.
-void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
-                    const lsjk::PairList* pl34, const double* const* Dpure, bool d24symm, bool flip_ok,
+// pointers in and out. Over twins D24 lives in the twins' slots of bases 2
+// and 4, while K13 is accumulated straight into the Cartesian spaces of the
+// caller's bases 1 and 3 (each partner primitive carries its output targets).
+void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12_in,
+                    const lsjk::PairList* pl34_in, const double* const* Dpure, bool d24symm, bool flip_ok,
                     double* const* Kpure, int ng, float thresp, float thredp)
 {
+    const lsjk::PairList* pl12 = effective(ctx, pl12_in);
+    const lsjk::PairList* pl34 = effective(ctx, pl34_in);
     ctx->scratch_reset();
-    const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    const lsjk::Basis *b1 = pl12_in->b1, *b2 = pl12->b2, *b3 = pl34_in->b1, *b4 = pl34->b2;
     double* Dc[lsjk::kJBatchMax];
     double* Kc[lsjk::kJBatchMax];
     for (int g = 0; g < ng; ++g) {
@@ -145,8 +176,11 @@ void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairL
         lsjk::pure_to_cart(ctx, b2, b4, Dpure[g], Dc[g]);
         LSJK_CUDA(cudaMemsetAsync(Kc[g], 0, sizeof(double) * b1->ncart * b3->ncart, ctx->stream));
     }
+    double* Ds[lsjk::kJBatchMax];
+    screening_densities(ctx, pl12_in->b2, pl34_in->b2, b2, b4, Dpure, ng, Ds);
     if (!ew.alpha.empty() && pl12->npair && pl34->npair)
-        lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Kc, ng, d24symm, flip_ok, thresp, thredp);
+        lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Ds[0] ? Ds : nullptr, Kc, ng, d24symm, flip_ok, thresp,
+                             thredp, b1, b3);
     for (int g = 0; g < ng; ++g) lsjk::cart_to_pure_acc(ctx, b1, b3, Kc[g], Kpure[g]);
 }
 
@@ -163,8 +197,10 @@ void exchange_prepare(lsjk::Context* ctx, lsjk::PairList* pl12, lsjk::PairList* 
     // the transposed write needs basis 1 == basis 3 as well (exchange.cpp:79-81)
     *flip = symm && pl12->b1->equivalent(*pl34->b1);
     *d24 = *flip;
-    lsjk::build_kinv(ctx, pl12);
-    if (pl34 != pl12) lsjk::build_kinv(ctx, pl34);
+    lsjk::PairList* e12 = const_cast<lsjk::PairList*>(effective(ctx, pl12));
+    lsjk::PairList* e34 = const_cast<lsjk::PairList*>(effective(ctx, pl34));
+    lsjk::build_kinv(ctx, e12);
+    if (e34 != e12) lsjk::build_kinv(ctx, e34);
 }
 
 // FMA throughput probe: 8 independent dependency chains per thread so the
@@ -283,6 +319,14 @@ int lsjk_context_destroy(lsjk_context* ctx)
         cudaStream_t s = ctx->c.stream;
         delete ctx;
         if (s) cudaStreamDestroy(s);
+    });
+}
+
+int lsjk_context_set_merge(lsjk_context* ctx, int on)
+{
+    return guard([&] {
+        if (!ctx) throw lsjk::Error(LSJK_EINVAL, "null context");
+        ctx->c.merge = on != 0;
     });
 }
 
@@ -444,6 +488,7 @@ int lsjk_basis_create(lsjk_context* ctx, int nprim, const double* c, const doubl
         B.atom.assign(atomIdx, atomIdx + nprim);
         try {
             lsjk::basis_init(&ctx->c, &B);
+            lsjk::basis_build_twin(&ctx->c, &B);
         } catch (...) {
             delete h;
             throw;
@@ -486,6 +531,17 @@ int lsjk_pairlist_build_schwarz(lsjk_context* ctx, const lsjk_basis* basis1, con
         P.thre = thre;
         try {
             lsjk::build_pairlist(&ctx->c, &P);
+            // the same list over the merged twins, for builds in merge mode
+            if (P.b1->twin || P.b2->twin) {
+                P.twin.reset(new lsjk::PairList());
+                lsjk::PairList& T = *P.twin;
+                T.ctx = &ctx->c;
+                T.b1 = P.b1->twin ? P.b1->twin.get() : P.b1;
+                T.b2 = P.b2->twin ? P.b2->twin.get() : P.b2;
+                T.symm = P.symm;
+                T.thre = P.thre;
+                lsjk::build_pairlist(&ctx->c, &T);
+            }
         } catch (...) {
             delete h;
             throw;

@@ -78,11 +78,19 @@ struct DBuf {
 
 struct Context;
 
-// Primitive data on the device (SoA).
+// Primitive data on the device (SoA). For the K kernels each primitive also
+// names where its contributions go in the output (Cartesian) matrix: up to two
+// target shells t0, t1 (Cartesian offsets; t1 = -1 if none) with weights w0,
+// w1, and `seg`, the id of the group of primitives that share those targets.
+// For a basis as given: t0 = cartIdx, t1 = -1, w0 = 1, seg = shellIdx. For a
+// merged basis (see Basis::twin) one primitive stands for the copies of an s
+// exponent that several contracted shells of an atom share.
 struct BasisView {
     int nprim, nao, ncart;
     const double *c, *e, *x, *y, *z;
     const int *L, *cart, *ao;
+    const int *t0, *t1, *seg;
+    const double *w0, *w1;
 };
 
 struct Basis {
@@ -92,14 +100,32 @@ struct Basis {
     // host copies
     std::vector<double> c, e, x, y, z;
     std::vector<int> L, pure, ao, cart, prim, shell, atom;
+    // output targets of each primitive (see BasisView)
+    std::vector<int> t0, t1, seg;
+    std::vector<double> w0, w1;
     // device copies
     DBuf<double> dc, de, dx, dy, dz;
     DBuf<int> dL, dcart, dao;
+    DBuf<int> dt0, dt1, dseg;
+    DBuf<double> dw0, dw1;
     // pure <-> cart maps: cart row -> (pure index, coef) and pure row -> (cart index, coef)
     DBuf<int> c2p_off, c2p_idx, p2c_off, p2c_idx;
     DBuf<double> c2p_w, p2c_w;
+    // per Cartesian slot of a twin: the Cartesian functions of the original basis
+    // it stands for (second -1 if none) and their weights (screening densities)
+    DBuf<int> uc_t0, uc_t1;
+    DBuf<double> uc_w0, uc_w1;
+    // The merged twin (null when no exponent is shared): one primitive per
+    // distinct (atom, s exponent), with c = the largest |c| of its copies,
+    // its own Cartesian slot, and pure <-> cart maps into THIS basis' AO
+    // space that carry the copies' contraction weights c_copy / c. J and K
+    // built over the twin equal the builds over this basis: every copy's
+    // integral is the twin primitive's times its weight.
+    std::unique_ptr<Basis> twin;
+    bool is_twin = false;   // this basis is a merged twin (some s primitives carry two targets)
     BasisView view() const {
-        return BasisView{nprim, nao, ncart, dc.p, de.p, dx.p, dy.p, dz.p, dL.p, dcart.p, dao.p};
+        return BasisView{nprim, nao, ncart, dc.p, de.p, dx.p, dy.p, dz.p, dL.p, dcart.p, dao.p,
+                         dt0.p, dt1.p, dseg.p, dw0.p, dw1.p};
     }
     bool equivalent(const Basis& o) const;
 };
@@ -133,8 +159,11 @@ struct KInvData {
     long nent = 0;
     DBuf<double> kab, p, ip, px, py, pz, ax, ay, az;        // FP64 pair data; kab = K_ab / p
     DBuf<float> kab32, p32, ip32, px32, py32, pz32, ax32, ay32, az32;  // FP32 copies
-    DBuf<int> pcart;                   // partner cartIdx
+    DBuf<int> pcart;                   // partner's first output target (t0; its cartIdx unless merged)
     DBuf<float> pbound;                // Schwarz bound of the pair
+    DBuf<int> pt1, pseg;               // partner's second target (-1: none) and target group
+    DBuf<double> pw0, pw1;             // partner's weights in its targets
+    DBuf<float> pw0_32, pw1_32;
 };
 
 struct PairList {
@@ -158,6 +187,8 @@ struct PairList {
     KInvData kdat;     // rows grouped by contracted shell (segments): the partner-1 side of K
     KInvData kdat_b;   // the same rows, entries by bound only: the partner-3 side of K
     bool kinv_built = false;
+    // the same list over the merged twins of b1 and b2 (null when neither has one)
+    std::unique_ptr<PairList> twin;
 };
 
 // Launch schedules picked by the autotuner (0 = built-in default).
@@ -197,6 +228,10 @@ struct Context {
     void scratch_reset() { scratch_used = 0; }
     int smem_optin = 0;
     int nsm = 148;                  // multiprocessors of the device
+    // build K over the merged twins of the bases (shared s exponents computed
+    // once); off (the default): over the primitives as given, the reference's
+    // exact quartet set. J always runs over the primitives as given.
+    bool merge = false;
 };
 
 // Stream-ordered scratch: a bump allocator over a few large blocks, reset at
@@ -255,11 +290,19 @@ inline T* take(Context* ctx, size_t n) { return reinterpret_cast<T*>(ctx->scratc
 
 // Build steps (basis.cu, pairs.cu, jbuild.cu, kbuild.cu)
 void basis_init(Context* ctx, Basis* B);
+// Build B->twin (left null when B shares no exponent between shells).
+void basis_build_twin(Context* ctx, Basis* B);
 double j_quartet_flops(int LB, int LK);
 double k_quartet_flops(int L1, int L2, int L3, int L4);
 void build_pairlist(Context* ctx, PairList* pl);
 void build_kinv(Context* ctx, PairList* pl);
 void pure_to_cart(Context* ctx, const Basis* b1, const Basis* b2, const double* Dpure, double* Dcart);
+// Screening density of twins u1 x u2 (u1/u2 may be plain bases) from the
+// Cartesian density Dorig of the bases they stand for (leading dimension ld):
+//   Dscr[a, b] = max over the copies (i of a, j of b) of |w_i w_j| |Dorig[i, j]|,
+// an upper bound of every copy's |D| weighted as the reference's screens see
+// it, so screens over twins keep every quartet the reference keeps.
+void screen_density(Context* ctx, const Basis* u1, const Basis* u2, const double* Dorig, int ld, double* Dscr);
 void cart_to_pure_acc(Context* ctx, const Basis* b1, const Basis* b2, const double* Xcart, double* Xpure);
 
 struct Ewald {
@@ -275,8 +318,13 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
                    const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp);
 // K for ng (1..4) densities sharing one task list (screened with the largest
 // |D24| of the batch) and the quartet integrals.
+// Dscr: the densities the screens read (Dcart itself when null, or screening
+// densities of the same layout when the pair lists are twins).
+// Kcart is laid out in the Cartesian spaces of kb1 x kb3, the bases the
+// partner primitives' output targets point into (pl12->b1 and pl34->b1
+// themselves, or the bases they are the twins of).
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                    const double* const* Dcart, double* const* Kcart, int ng, bool d24symm, bool flip_ok,
-                    float thresp, float thredp);
+                    const double* const* Dcart, const double* const* Dscr, double* const* Kcart, int ng,
+                    bool d24symm, bool flip_ok, float thresp, float thredp, const Basis* kb1, const Basis* kb3);
 
 } // namespace lsjk

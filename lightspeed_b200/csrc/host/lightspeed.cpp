@@ -256,6 +256,12 @@ void Engine::set_precision(int mode)
     precision_ = mode;
 }
 
+void Engine::set_merge(bool on)
+{
+    check_rc(lsjk_context_set_merge(ctx_, on ? 1 : 0), "Engine::set_merge");
+    merge_ = on;
+}
+
 std::shared_ptr<ResourceList> ResourceList::build(size_t, size_t)
 {
     Engine::instance();

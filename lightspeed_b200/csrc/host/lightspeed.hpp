@@ -174,12 +174,15 @@ public:
     int device() const { return device_; }
     void set_precision(int mode);
     int precision() const { return precision_; }
+    void set_merge(bool on);
+    bool merge() const { return merge_; }
 
 private:
     Engine();
     lsjk_context* ctx_ = nullptr;
     int device_ = 0;
     int precision_ = LSJK_PREC_MIXED;
+    bool merge_ = false;
 };
 
 class ResourceList {

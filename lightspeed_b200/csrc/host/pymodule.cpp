@@ -198,6 +198,10 @@ PYBIND11_MODULE(_lightspeed, m)
     m.attr("PREC_MIXED") = LSJK_PREC_MIXED;
     m.attr("PREC_FP64") = LSJK_PREC_FP64;
     m.def("set_precision", [](int mode) { Engine::instance().set_precision(mode); });
+    m.def("set_merge", [](bool on) { Engine::instance().set_merge(on); },
+          "K over merged twins of the bases (shared s exponents computed once) or, the default, over the "
+          "primitives as given (the reference's exact quartet set); J always runs over the primitives as given");
+    m.def("get_merge", []() { return Engine::instance().merge(); });
     m.def("get_precision", []() { return Engine::instance().precision(); });
     m.def("stats", &stats_dict);
     m.def("flops_split", []() {
@@ -274,6 +278,7 @@ PYBIND11_MODULE(_lightspeed, m)
         {
             check_rc(lsjk_context_create(device, &c), "Stream");
             check_rc(lsjk_context_set_precision(c, Engine::instance().precision()), "Stream");
+            check_rc(lsjk_context_set_merge(c, Engine::instance().merge() ? 1 : 0), "Stream");
         }
         ~ExtraContext() { if (c) lsjk_context_destroy(c); }
     };
@@ -281,6 +286,8 @@ PYBIND11_MODULE(_lightspeed, m)
         .def(py::init([]() { return std::make_shared<ExtraContext>(Engine::instance().device()); }))
         .def("set_precision", [](ExtraContext& x, int mode) { check_rc(lsjk_context_set_precision(x.c, mode),
                                                                        "Stream.set_precision"); })
+        .def("set_merge", [](ExtraContext& x, bool on) { check_rc(lsjk_context_set_merge(x.c, on ? 1 : 0),
+                                                                   "Stream.set_merge"); })
         .def("stream_handle", [](ExtraContext& x) { return (uintptr_t) lsjk_context_stream(x.c); })
         .def("stats", [](ExtraContext& x) { return stats_dict_of(x.c); })
         .def("reset_stats", [](ExtraContext& x) { check_rc(lsjk_context_reset_stats(x.c), "Stream.reset_stats"); })

@@ -23,10 +23,11 @@ struct KScalars {
     float thre12, thre34;
 };
 
-// K-invert partner data of one pair list, in one precision.
+// K-invert partner data of one pair list, in one precision (w0, w1: the
+// partner's weights in its two output targets).
 template <typename R>
 struct KRows {
-    const R *kab, *p, *ip, *px, *py, *pz, *ax, *ay, *az;
+    const R *kab, *p, *ip, *px, *py, *pz, *ax, *ay, *az, *w0, *w1;
 };
 
 struct KArgs {
@@ -39,17 +40,26 @@ struct KArgs {
     const int* r34l;
     KRows<double> d12, d34;
     KRows<float> f12, f34;
+    // partner output targets: first (t0) and second (t1, -1 if none) Cartesian
+    // offsets, and the target group that delimits a partner-1 segment
     const int* cart12;
+    const int* t1_12;
+    const int* seg12;
     const float* b12;
     const int* cart34;
+    const int* t1_34;
+    const double* w0_34;      // partner-3 weights in FP64 (applied when a segment is flushed)
+    const double* w1_34;
     const float* b34;
     BasisView b2, b4;         // indexed primitives (centres, cartIdx)
     const double* Dc[kKBatch];   // D24 of each density of the launch (Cartesian, ld4)
     int ld4;
-    double* Kc[kKBatch];         // K13 of each density (Cartesian, ld3)
+    double* Kc[kKBatch];         // K13 of each density (Cartesian output space of bases 1 and 3, ld3)
     int ld3;
     int ng;                      // densities: launch_k splits them over kernel launches
     int flip;
+    int gc;                      // partners may carry two output targets (merged twins): the kernel
+                                 // variant with two target blocks for s-type partners
     // this pass computes quartets with thr_lo <= estimate < thr_hi
     float thr_lo, thr_hi;
     const KScalars* sc;

@@ -215,19 +215,21 @@ double k_quartet_flops(int L1, int L2, int L3, int L4)
 }
 
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                    const double* const* Dcart, double* const* Kcart, int ng, bool d24symm, bool flip_ok,
-                    float thresp, float thredp)
+                    const double* const* Dcart, const double* const* Dscr_in, double* const* Kcart, int ng,
+                    bool d24symm, bool flip_ok, float thresp, float thredp, const Basis* kb1, const Basis* kb3)
 {
+    // screens read Dscr (max|D24| estimates); the integrals contract with Dcart
+    const double* const* Dscr = Dscr_in ? Dscr_in : Dcart;
     if (ng < 1 || ng > kKBatch) throw Error(LSJK_EINVAL, "exchange_build: 1..4 densities per build");
     cudaStream_t s = ctx->stream;
-    const int b1c = pl12->b1->ncart;
-    const Basis *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    const int b1c = kb1->ncart;   // K13 lives in the output spaces of bases 1 and 3
+    const Basis *b2 = pl12->b2, *b3 = kb3, *b4 = pl34->b2;
     // global max |D24| (exchange.cpp:48-52) and the K-invert thresholds
     KScalars* sc = take<KScalars>(ctx, 1);
     LSJK_CUDA(cudaMemsetAsync(sc, 0, sizeof(KScalars), s));
     long nd = (long) pl12->b2->ncart * b4->ncart;
     for (int g = 0; g < ng && nd; ++g) {
-        k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(Dcart[g], nd, &sc->dmax_bits);
+        k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(Dscr[g], nd, &sc->dmax_bits);
         ctx->stats.kernel_launches++;
     }
     k_kscalars<<<1, 1, 0, s>>>(sc, thresp, pl12->max_bound, pl34->max_bound);
@@ -269,7 +271,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
         }
     G.pb12 = pl12->kdat.pbound.p;
     G.pb34 = pl34->kdat.pbound.p;
-    for (int g = 0; g < ng; ++g) G.Dc[g] = Dcart[g];
+    for (int g = 0; g < ng; ++g) G.Dc[g] = Dscr[g];
     G.ng = ng;
     G.ld4 = b4->ncart;
     G.d24symm = d24symm ? 1 : 0;
@@ -317,16 +319,23 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     const KInvData& d12 = pl12->kdat;     // partner 1: shell segments
                     const KInvData& d34 = pl34->kdat_b;   // partner 3: by bound
                     A.d12 = KRows<double>{d12.kab.p, d12.p.p, d12.ip.p, d12.px.p, d12.py.p, d12.pz.p,
-                                          d12.ax.p, d12.ay.p, d12.az.p};
+                                          d12.ax.p, d12.ay.p, d12.az.p, d12.pw0.p, d12.pw1.p};
                     A.d34 = KRows<double>{d34.kab.p, d34.p.p, d34.ip.p, d34.px.p, d34.py.p, d34.pz.p,
-                                          d34.ax.p, d34.ay.p, d34.az.p};
+                                          d34.ax.p, d34.ay.p, d34.az.p, d34.pw0.p, d34.pw1.p};
                     A.f12 = KRows<float>{d12.kab32.p, d12.p32.p, d12.ip32.p, d12.px32.p, d12.py32.p,
-                                         d12.pz32.p, d12.ax32.p, d12.ay32.p, d12.az32.p};
+                                         d12.pz32.p, d12.ax32.p, d12.ay32.p, d12.az32.p, d12.pw0_32.p,
+                                         d12.pw1_32.p};
                     A.f34 = KRows<float>{d34.kab32.p, d34.p32.p, d34.ip32.p, d34.px32.p, d34.py32.p,
-                                         d34.pz32.p, d34.ax32.p, d34.ay32.p, d34.az32.p};
+                                         d34.pz32.p, d34.ax32.p, d34.ay32.p, d34.az32.p, d34.pw0_32.p,
+                                         d34.pw1_32.p};
                     A.cart12 = d12.pcart.p;
+                    A.t1_12 = d12.pt1.p;
+                    A.seg12 = d12.pseg.p;
                     A.b12 = d12.pbound.p;
                     A.cart34 = d34.pcart.p;
+                    A.t1_34 = d34.pt1.p;
+                    A.w0_34 = d34.pw0.p;
+                    A.w1_34 = d34.pw1.p;
                     A.b34 = d34.pbound.p;
                     A.b2 = b2->view();
                     A.b4 = b4->view();
@@ -338,6 +347,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     A.ld4 = b4->ncart;
                     A.ld3 = b3->ncart;
                     A.flip = flip_ok ? 1 : 0;
+                    A.gc = (pl12->b1->is_twin || pl34->b1->is_twin) ? 1 : 0;
                     A.sc = sc;
                     A.nbin = kRysNbin[NR];
                     A.tmax = kRysTmax[NR];

@@ -45,12 +45,14 @@ __device__ __forceinline__ float float_threshold(double thr, double dmax)
     return x;
 }
 
-// One partner-1 entry as staged in shared memory (80 / 48 bytes).
+// One partner-1 entry as staged in shared memory (112 / 64 bytes): pair data,
+// the partner's weights in its two output targets, the bound, the first and
+// second target (Cartesian offsets, t1 = -1 if none) and the target group.
 template <typename R>
 struct alignas(16) KEnt {
-    R kab, p, ip, px, py, pz, ax, ay, az;
+    R kab, p, ip, px, py, pz, ax, ay, az, w0, w1;
     float b;
-    int c;
+    int c, t1, seg;
 };
 
 // Tasks a warp takes from the queue at once (at most; fewer when the class
@@ -72,7 +74,8 @@ struct alignas(16) KHdr {
 // Lane l copies entry kb + l of the row (if it exists) into dst[l].
 template <typename R>
 __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const float* __restrict__ b,
-                                          const int* __restrict__ cart, int s12, int kb, int n12, int lane)
+                                          const int* __restrict__ cart, const int* __restrict__ t1,
+                                          const int* __restrict__ seg, int s12, int kb, int n12, int lane)
 {
     if (kb + lane >= n12) return;
     const int e = s12 + kb + lane;
@@ -87,6 +90,8 @@ __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const
         cp_async8(&o->ax, d.ax + e);
         cp_async8(&o->ay, d.ay + e);
         cp_async8(&o->az, d.az + e);
+        cp_async8(&o->w0, d.w0 + e);
+        cp_async8(&o->w1, d.w1 + e);
     } else {
         cp_async4(&o->kab, d.kab + e);
         cp_async4(&o->p, d.p + e);
@@ -97,9 +102,13 @@ __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const
         cp_async4(&o->ax, d.ax + e);
         cp_async4(&o->ay, d.ay + e);
         cp_async4(&o->az, d.az + e);
+        cp_async4(&o->w0, d.w0 + e);
+        cp_async4(&o->w1, d.w1 + e);
     }
     cp_async4(&o->b, b + e);
     cp_async4(&o->c, cart + e);
+    cp_async4(&o->t1, t1 + e);
+    cp_async4(&o->seg, seg + e);
 }
 
 // Densities per launch for a class: up to kKBatch while a per-density
@@ -157,12 +166,12 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
             if (T < tmax - tmax / (R) A.nbin) {
                 rys_eval<NR, R>(T, tab, A.nbin, tmax, asym_t, asym_w, t2, w);
             } else {
-                const double r = rsqrt((double) rho * (double) d2 * (double) RR);
+                const double r = rsqrt_f64_newton((double) rho * (double) d2 * (double) RR);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
-                    const double t = A.asym64_t[i] * r;
+                    const double t = c_rys_asym_t[NR * LSJK_RYS_NMAX + i] * r;
                     t2[i] = (R) (t * t);
-                    w[i] = (R) (A.asym64_w[i] * r);
+                    w[i] = (R) (c_rys_asym_w[NR * LSJK_RYS_NMAX + i] * r);
                 }
             }
         } else {
@@ -199,12 +208,16 @@ __device__ __forceinline__ void k_quartet(const KArgs& A, const R* __restrict__ 
     }
 }
 
-template <int L1, int L2, int L3, int L4, typename R, int NG>
+template <int L1, int L2, int L3, int L4, typename R, int NG, bool GC>
 __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ KArgs A)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
     constexpr bool FP64 = std::is_same<R, double>::value;
+    // over merged twins s-type partners may stand for two contracted shells:
+    // two target blocks per segment (partner 1) or per lane (partner 3)
+    constexpr int G1 = (GC && L1 == 0) ? 2 : 1;
+    constexpr int G3 = (GC && L3 == 0) ? 2 : 1;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R* tab = reinterpret_cast<R*>(smem_raw);
     __shared__ __align__(8) uint64_t mbar;
@@ -292,13 +305,19 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                 const bool in3 = cs + lane < n34;
                 float b34 = 0.0f;
                 R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
-                int c3 = 0;
+                int c3 = 0, c3b = -1;
+                double w30 = 1.0, w31 = 0.0;
                 if (in3) {
                     b34 = A.b34[k3];
                     kab34 = d34.kab[k3]; q = d34.p[k3]; iq = d34.ip[k3];
                     Qx = d34.px[k3]; Qy = d34.py[k3]; Qz = d34.pz[k3];
                     Cx = d34.ax[k3]; Cy = d34.ay[k3]; Cz = d34.az[k3];
                     c3 = A.cart34[k3];
+                    if constexpr (G3 == 2) {
+                        c3b = A.t1_34[k3];
+                        w30 = A.w0_34[k3];
+                        w31 = A.w1_34[k3];
+                    }
                 }
                 const bool v3 = in3 && b34 >= thre34;
                 if (!v3) b34 = 0.0f;
@@ -310,16 +329,22 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                 for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
                 // partners 3 come by bound: no later chunk passes either
                 if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
+                // segment accumulators: acc for the segment's first target, accb for its
+                // second (s-type partners 1 may stand for two contracted shells)
                 R acc[NG][N1 * N3];
+                R accb[NG][G1 == 2 ? N1 * N3 : 1];
 #pragma unroll
-                for (int g = 0; g < NG; ++g)
+                for (int g = 0; g < NG; ++g) {
 #pragma unroll
                     for (int t = 0; t < N1 * N3; ++t) acc[g][t] = R(0);
+#pragma unroll
+                    for (int t = 0; t < (G1 == 2 ? N1 * N3 : 1); ++t) accb[g][t] = R(0);
+                }
                 bool any = false;
-                int prev_c1 = -1;
-                // flush the finished shell segment of partner 1: one atomic per element and density
-                // (fire-and-forget reductions; a segmented shuffle sum over the lanes of one shell 3
-                // before them measured slower)
+                int prev_seg = -1, prev_c1 = 0, prev_c1b = -1;
+                // flush the finished shell segment of partner 1: one atomic per element, density
+                // and target pair (fire-and-forget reductions; a segmented shuffle sum over the
+                // lanes of one shell 3 before them measured slower)
                 auto flush = [&]() {
                     if (any) {
 #pragma unroll
@@ -329,33 +354,57 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                             for (int a = 0; a < N1; ++a)
 #pragma unroll
                                 for (int c = 0; c < N3; ++c) {
-                                    atomicAdd(&Kc[(long) (prev_c1 + a) * A.ld3 + c3 + c], wsym * (double) acc[g][a * N3 + c]);
+                                    const double v = wsym * (double) acc[g][a * N3 + c];
+                                    double* row = Kc + (long) (prev_c1 + a) * A.ld3;
+                                    if constexpr (G3 == 2) {
+                                        atomicAdd(row + c3 + c, w30 * v);
+                                        if (c3b >= 0) atomicAdd(row + c3b + c, w31 * v);
+                                    } else {
+                                        atomicAdd(row + c3 + c, v);
+                                    }
                                     acc[g][a * N3 + c] = R(0);
+                                    if constexpr (G1 == 2) {
+                                        if (prev_c1b >= 0) {
+                                            const double vb = wsym * (double) accb[g][a * N3 + c];
+                                            double* rowb = Kc + (long) (prev_c1b + a) * A.ld3;
+                                            if constexpr (G3 == 2) {
+                                                atomicAdd(rowb + c3 + c, w30 * vb);
+                                                if (c3b >= 0) atomicAdd(rowb + c3b + c, w31 * vb);
+                                            } else {
+                                                atomicAdd(rowb + c3 + c, vb);
+                                            }
+                                        }
+                                        accb[g][a * N3 + c] = R(0);
+                                    }
                                 }
                         }
                     }
                     any = false;
                 };
-                stage_ent(ring, d12, A.b12, A.cart12, s12, 0, n12, lane);
+                stage_ent(ring, d12, A.b12, A.cart12, A.t1_12, A.seg12, s12, 0, n12, lane);
                 cp_async_commit();
                 bool stop = false;
                 for (int kb = 0; kb < n12 && !stop; kb += 32) {
                     const KEnt<R>* cur = ring + ((kb >> 5) & 1) * 32;
-                    if (kb + 32 < n12) stage_ent(ring + (((kb >> 5) + 1) & 1) * 32, d12, A.b12, A.cart12, s12, kb + 32, n12, lane);
+                    if (kb + 32 < n12)
+                        stage_ent(ring + (((kb >> 5) + 1) & 1) * 32, d12, A.b12, A.cart12, A.t1_12, A.seg12, s12,
+                                  kb + 32, n12, lane);
                     cp_async_commit();
                     cp_async_wait<1>();
                     __syncwarp();
                     const int kend = min(32, n12 - kb);
                     // chg bit l: entry l of the chunk starts a new shell segment (l >= 1)
-                    const int cl = lane < kend ? cur[lane].c : -1;
+                    const int cl = lane < kend ? cur[lane].seg : -1;
                     const int cl_prev = __shfl_up_sync(0xffffffffu, cl, 1);
                     const unsigned chg = __ballot_sync(0xffffffffu, lane >= 1 && lane < kend && cl != cl_prev);
                     for (int j = 0; j < kend; ++j) {
                         const float b12 = cur[j].b;
-                        const int c1 = cur[j].c;
-                        if (c1 != prev_c1) {
+                        const int sg = cur[j].seg;
+                        if (sg != prev_seg) {
                             flush();
-                            prev_c1 = c1;
+                            prev_seg = sg;
+                            prev_c1 = cur[j].c;
+                            if constexpr (G1 == 2) prev_c1b = cur[j].t1;
                             // segments are ordered by their largest bound: nothing later passes
                             if (b12 < thre12 || b12 * bmax34 < tlo) {
                                 stop = true;
@@ -375,8 +424,26 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                         const KEnt<R> e = cur[j];
                         ++nq;
                         any = true;
-                        k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy, Sz, QCx,
-                                                         QCy, QCz, Cx, Cy, Cz, Dblk, acc);
+                        if constexpr (G1 == 2) {
+                            // one integral, added to both targets with the entry's weights
+                            R tmp[NG][N1 * N3];
+#pragma unroll
+                            for (int g = 0; g < NG; ++g)
+#pragma unroll
+                                for (int t = 0; t < N1 * N3; ++t) tmp[g][t] = R(0);
+                            k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy,
+                                                             Sz, QCx, QCy, QCz, Cx, Cy, Cz, Dblk, tmp);
+#pragma unroll
+                            for (int g = 0; g < NG; ++g)
+#pragma unroll
+                                for (int t = 0; t < N1 * N3; ++t) {
+                                    acc[g][t] = fma(e.w0, tmp[g][t], acc[g][t]);
+                                    accb[g][t] = fma(e.w1, tmp[g][t], accb[g][t]);
+                                }
+                        } else {
+                            k_quartet<L1, L2, L3, L4, R, NG>(A, tab, tmax, asym_t, asym_w, e, kab34, q, iq, Sx, Sy,
+                                                             Sz, QCx, QCy, QCz, Cx, Cy, Cz, Dblk, acc);
+                        }
                     }
                     __syncwarp();   // the next chunk's prefetch refills this slot
                 }
@@ -390,7 +457,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     if (lane == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
 }
 
-template <int L1, int L2, int L3, int L4, typename R, int NG>
+template <int L1, int L2, int L3, int L4, typename R, int NG, bool GC>
 void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
 {
     constexpr int NR = (L1 + L2 + L3 + L4) / 2 + 1;
@@ -401,21 +468,33 @@ void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
     static std::atomic<int> resident[64];
     const int dev = ctx->device & 63;
     const unsigned long long bit = 1ull << dev;
+    auto kern = k_exchange<L1, L2, L3, L4, R, NG, GC>;
     if (!(attr_devices.load(std::memory_order_acquire) & bit)) {
-        LSJK_CUDA(cudaFuncSetAttribute(k_exchange<L1, L2, L3, L4, R, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int) smem));
+        LSJK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         int occ = 0;
-        LSJK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exchange<L1, L2, L3, L4, R, NG>, kKThreads,
-                                                                smem));
+        LSJK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kKThreads, smem));
         resident[dev].store(occ > 0 ? occ : 1, std::memory_order_relaxed);
         attr_devices.fetch_or(bit, std::memory_order_acq_rel);
     }
     // warps take tasks from the queue until it is empty, so CTAs beyond one
     // resident wave would only start, find no work and leave
     grid = std::min<unsigned>(grid, (unsigned) (ctx->nsm * resident[dev].load(std::memory_order_relaxed)));
-    k_exchange<L1, L2, L3, L4, R, NG><<<grid, kKThreads, smem, ctx->stream>>>(A);
+    kern<<<grid, kKThreads, smem, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
+}
+
+// The two-target variant only where an s-type partner can carry two targets.
+template <int L1, int L2, int L3, int L4, typename R, int NG>
+void launch_k_gc(Context* ctx, const KArgs& A, unsigned grid)
+{
+    if constexpr (L1 == 0 || L3 == 0) {
+        if (A.gc) {
+            launch_k_one<L1, L2, L3, L4, R, NG, true>(ctx, A, grid);
+            return;
+        }
+    }
+    launch_k_one<L1, L2, L3, L4, R, NG, false>(ctx, A, grid);
 }
 
 // One class, one precision pass, A.ng densities: launches of k_batch densities
@@ -440,19 +519,19 @@ void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
         if (fp32) {
             constexpr int NGf = k_batch<L1, L2, L3, L4, float>();
             if (NGf > 1 && A.ng - g0 >= NGf) {
-                launch_k_one<L1, L2, L3, L4, float, NGf>(ctx, B, grid);
+                launch_k_gc<L1, L2, L3, L4, float, NGf>(ctx, B, grid);
                 used = NGf;
             } else {
-                launch_k_one<L1, L2, L3, L4, float, 1>(ctx, B, grid);
+                launch_k_gc<L1, L2, L3, L4, float, 1>(ctx, B, grid);
                 used = 1;
             }
         } else {
             constexpr int NGd = k_batch<L1, L2, L3, L4, double>();
             if (NGd > 1 && A.ng - g0 >= NGd) {
-                launch_k_one<L1, L2, L3, L4, double, NGd>(ctx, B, grid);
+                launch_k_gc<L1, L2, L3, L4, double, NGd>(ctx, B, grid);
                 used = NGd;
             } else {
-                launch_k_one<L1, L2, L3, L4, double, 1>(ctx, B, grid);
+                launch_k_gc<L1, L2, L3, L4, double, 1>(ctx, B, grid);
                 used = 1;
             }
         }

@@ -126,6 +126,23 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Half-range Gauss-Hermite nodes and weights of the asymptotic Rys rules,
+// [nrys][root], in constant memory (read with uniform indices).
+static __constant__ double c_rys_asym_t[(LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX] = {LSJK_RYS_ASYM_T_LIST};
+static __constant__ double c_rys_asym_w[(LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX] = {LSJK_RYS_ASYM_W_LIST};
+
+// 1/sqrt(T) in FP64 for T > 0: the FP32 estimate refined by two Newton steps
+// r <- r (3 - T r^2) / 2 (relative error ~1e-16; the FP32 paths' switch
+// region never sees T near 0 or beyond the float range).
+__device__ __forceinline__ double rsqrt_f64_newton(double T)
+{
+    double r = (double) rsqrtf((float) T);
+    const double hT = 0.5 * T;
+    r = r * fma(-hT * r, r, 1.5);
+    r = r * fma(-hT * r, r, 1.5);
+    return r;
+}
+
 __device__ __forceinline__ double dexp(double x) { return exp(x); }
 __device__ __forceinline__ float dexp(float x) { return __expf(x); }
 __device__ __forceinline__ double drsqrt(double x) { return rsqrt(x); }
@@ -166,8 +183,9 @@ __device__ __forceinline__ void boys_eval(R T, const R* __restrict__ tab, R* __r
 }
 
 // Rys roots (returned as t^2) and weights of the N-point rule at T. `tab` is the
-// per-rule block [2N][nbin][8] (roots t, then ln w); `asym_t/asym_w` hold the
-// half-range Gauss-Hermite limit used for T >= tmax.
+// per-rule block [2N][nbin][8] (roots t, then ln w; for N = 1 the weight
+// w = F_0(T) itself, so the one-root classes need no exponential);
+// `asym_t/asym_w` hold the half-range Gauss-Hermite limit used for T >= tmax.
 template <int N, typename R>
 __device__ __forceinline__ void rys_eval(R T, const R* __restrict__ tab, int nbin, R tmax,
                                          const R* __restrict__ asym_t, const R* __restrict__ asym_w,
@@ -182,7 +200,8 @@ __device__ __forceinline__ void rys_eval(R T, const R* __restrict__ tab, int nbi
         for (int i = 0; i < N; ++i) {
             const R t = horner8(tab + 8 * (i * nbin + b), x);
             t2[i] = t * t;
-            w[i] = dexp(horner8(tab + 8 * ((N + i) * nbin + b), x));
+            const R lw = horner8(tab + 8 * ((N + i) * nbin + b), x);
+            w[i] = N == 1 ? lw : dexp(lw);
         }
     } else {
         const R r = drsqrt(T);
@@ -202,11 +221,13 @@ __device__ __forceinline__ void rys_eval(R T, const R* __restrict__ tab, int nbi
 template <int L>
 __device__ __forceinline__ void boys_asym_f64_to_f32(double T, float* __restrict__ F)
 {
-    const double r = rsqrt(T);
+    const double r = rsqrt_f64_newton(T);
     double f = 0.88622692545275801364908374167057259 * r;   // sqrt(pi)/2 / sqrt(T)
     F[0] = (float) f;
     if (L > 0) {
-        const double e = exp(-T);
+        // exp(-T) <= 3e-16 here: its relative size in F_m is below 1e-10, so its own
+        // FP32 rounding changes F_m by less than 1e-17 relative
+        const double e = (double) __expf(-(float) T);
         const double h = 0.5 * r * r;
 #pragma unroll
         for (int m = 0; m < L; ++m) {

@@ -172,14 +172,15 @@ __global__ void k_kinv_key1(const KEnt* __restrict__ e, long n, unsigned long lo
     val[k] = (int) k;
 }
 
-// pass B key: (class, indexed, partner cartIdx) -- the cartIdx names the contracted shell
+// pass B key: (class, indexed, partner target group) -- the group names the
+// output block(s) the partner's contributions go to (its contracted shell)
 __global__ void k_kinv_key2(const KEnt* __restrict__ e, const int* __restrict__ perm, long n,
-                            const int* __restrict__ pcart, unsigned long long* __restrict__ key)
+                            const int* __restrict__ pseg, unsigned long long* __restrict__ key)
 {
     long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
     if (k >= n) return;
     const KEnt& t = e[perm[k]];
-    key[k] = ((unsigned long long) t.cls << 48) | ((unsigned long long) t.idx << 32) | (unsigned) pcart[t.part];
+    key[k] = ((unsigned long long) t.cls << 48) | ((unsigned long long) t.idx << 32) | (unsigned) pseg[t.part];
 }
 
 // row key (class, indexed): a stable pass over the bound order gives each row
@@ -217,7 +218,9 @@ __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ 
                             float* __restrict__ kab32, float* __restrict__ pp32, float* __restrict__ ipp32,
                             float* __restrict__ px32, float* __restrict__ py32, float* __restrict__ pz32,
                             float* __restrict__ ax32, float* __restrict__ ay32, float* __restrict__ az32,
-                            int* __restrict__ pcart, float* __restrict__ pb,
+                            int* __restrict__ pcart, float* __restrict__ pb, int* __restrict__ pt1,
+                            int* __restrict__ pseg, double* __restrict__ pw0, double* __restrict__ pw1,
+                            float* __restrict__ pw0_32, float* __restrict__ pw1_32,
                             int* __restrict__ rstart, int* __restrict__ rlen, int nrow)
 {
     long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
@@ -235,7 +238,13 @@ __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ 
     kab32[k] = (float) (K * ip); pp32[k] = (float) p; ipp32[k] = (float) ip;
     px32[k] = (float) Px; py32[k] = (float) Py; pz32[k] = (float) Pz;
     ax32[k] = (float) Ax; ay32[k] = (float) Ay; az32[k] = (float) Az;
-    pcart[k] = bpart.cart[j];
+    pcart[k] = bpart.t0[j];
+    pt1[k] = bpart.t1[j];
+    pseg[k] = bpart.seg[j];
+    pw0[k] = bpart.w0[j];
+    pw1[k] = bpart.w1[j];
+    pw0_32[k] = (float) bpart.w0[j];
+    pw1_32[k] = (float) bpart.w1[j];
     pb[k] = t.b;
     long r = (long) t.cls * nrow + i;
     bool first = (k == 0);
@@ -388,6 +397,7 @@ void build_kinv(Context* ctx, PairList* pl)
     kd.kab32.alloc(m); kd.p32.alloc(m); kd.ip32.alloc(m); kd.px32.alloc(m); kd.py32.alloc(m);
     kd.pz32.alloc(m); kd.ax32.alloc(m); kd.ay32.alloc(m); kd.az32.alloc(m);
     kd.pcart.alloc(m); kd.pbound.alloc(m);
+    kd.pt1.alloc(m); kd.pseg.alloc(m); kd.pw0.alloc(m); kd.pw1.alloc(m); kd.pw0_32.alloc(m); kd.pw1_32.alloc(m);
     unsigned long long* ka = take<unsigned long long>(ctx, m);
     unsigned long long* kas = take<unsigned long long>(ctx, m);
     int* va = take<int>(ctx, m);
@@ -402,7 +412,7 @@ void build_kinv(Context* ctx, PairList* pl)
     unsigned long long* kb = take<unsigned long long>(ctx, m);
     unsigned long long* kbs = take<unsigned long long>(ctx, m);
     int* pb2 = take<int>(ctx, m);
-    k_kinv_key2<<<nblk(m, 256), 256, 0, s>>>(ent, pa, m, bpart->dcart.p, kb);
+    k_kinv_key2<<<nblk(m, 256), 256, 0, s>>>(ent, pa, m, bpart->dseg.p, kb);
     radix_sort_pairs(ctx, kb, kbs, pa, pb2, m, 52);
     unsigned long long* kc = take<unsigned long long>(ctx, m);
     unsigned long long* kcs = take<unsigned long long>(ctx, m);
@@ -417,7 +427,8 @@ void build_kinv(Context* ctx, PairList* pl)
     k_kinv_fill<<<nblk(m, 256), 256, 0, s>>>(ent, perm, m, bidx->view(), bpart->view(), nullptr, kd.kab.p, kd.p.p,
                                             kd.ip.p, kd.px.p, kd.py.p, kd.pz.p, kd.ax.p, kd.ay.p, kd.az.p,
                                             kd.kab32.p, kd.p32.p, kd.ip32.p, kd.px32.p, kd.py32.p, kd.pz32.p,
-                                            kd.ax32.p, kd.ay32.p, kd.az32.p, kd.pcart.p, kd.pbound.p, rstart,
+                                            kd.ax32.p, kd.ay32.p, kd.az32.p, kd.pcart.p, kd.pbound.p, kd.pt1.p,
+                                            kd.pseg.p, kd.pw0.p, kd.pw1.p, kd.pw0_32.p, kd.pw1_32.p, rstart,
                                             rlen, nrow);
     LSJK_CUDA(cudaGetLastError());
     // the bound-ordered copy (same rows, so the same row tables)
@@ -428,6 +439,8 @@ void build_kinv(Context* ctx, PairList* pl)
     kb_.kab32.alloc(m); kb_.p32.alloc(m); kb_.ip32.alloc(m); kb_.px32.alloc(m); kb_.py32.alloc(m);
     kb_.pz32.alloc(m); kb_.ax32.alloc(m); kb_.ay32.alloc(m); kb_.az32.alloc(m);
     kb_.pcart.alloc(m); kb_.pbound.alloc(m);
+    kb_.pt1.alloc(m); kb_.pseg.alloc(m); kb_.pw0.alloc(m); kb_.pw1.alloc(m); kb_.pw0_32.alloc(m);
+    kb_.pw1_32.alloc(m);
     int* rstart_b = take<int>(ctx, (long) kNL * kNL * nrow);
     int* rlen_b = take<int>(ctx, (long) kNL * kNL * nrow);
     LSJK_CUDA(cudaMemsetAsync(rstart_b, 0, sizeof(int) * kNL * kNL * nrow, s));
@@ -436,7 +449,8 @@ void build_kinv(Context* ctx, PairList* pl)
                                             kb_.p.p, kb_.ip.p, kb_.px.p, kb_.py.p, kb_.pz.p, kb_.ax.p, kb_.ay.p,
                                             kb_.az.p, kb_.kab32.p, kb_.p32.p, kb_.ip32.p, kb_.px32.p, kb_.py32.p,
                                             kb_.pz32.p, kb_.ax32.p, kb_.ay32.p, kb_.az32.p, kb_.pcart.p,
-                                            kb_.pbound.p, rstart_b, rlen_b, nrow);
+                                            kb_.pbound.p, kb_.pt1.p, kb_.pseg.p, kb_.pw0.p, kb_.pw1.p, kb_.pw0_32.p,
+                                            kb_.pw1_32.p, rstart_b, rlen_b, nrow);
     LSJK_CUDA(cudaGetLastError());
     for (int a = 0; a < kNL; ++a)
         for (int b = 0; b < kNL; ++b) {

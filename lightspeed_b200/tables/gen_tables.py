@@ -16,7 +16,9 @@ The tables are built here from first principles, not taken from any other code:
   uses F_0 = sqrt(pi/T)/2 and the upward recursion with the exp(-T) term.
 
 Each interval [0, T_asym) is split into uniform bins; in every bin each function
-(t_i, ln w_i for Rys; F_m for Boys) is interpolated by a degree-7 Chebyshev
+(t_i, ln w_i for Rys -- for the one-point rule w_1 = F_0(T) itself, smooth and
+of modest range, so the device needs no exponential there; F_m for Boys) is
+interpolated by a degree-7 Chebyshev
 series that is then rewritten as a monomial polynomial in the local variable
 x in [-1, 1] so the device can evaluate it with 8 fused multiply-adds (Horner).
 Interpolating ln w (then exponentiating) keeps small weights relatively
@@ -140,7 +142,7 @@ def build_rys(n, width):
 
     def func(T):
         t, w = rys_exact(n, T)
-        return np.concatenate([t, np.log(w)])
+        return np.concatenate([t, w if n == 1 else np.log(w)])
 
     coefs = _fit_bins(func, 2 * n, tmax, nbin)
     # accuracy check on random points
@@ -150,7 +152,7 @@ def build_rys(n, width):
         t, w = rys_exact(n, T)
         v = _eval_bins(coefs, tmax, nbin, T)
         errt = max(errt, np.max(np.abs(v[:n] - t)))
-        errw = max(errw, np.max(np.abs(np.exp(v[n:]) - w)))
+        errw = max(errw, np.max(np.abs((v[n:] if n == 1 else np.exp(v[n:])) - w)))
     return dict(n=n, tmax=tmax, nbin=nbin, coefs=coefs, asym=rys_asym(n), errt=errt, errw=errw)
 
 
@@ -180,7 +182,8 @@ def _fmt(a):
 
 def write_inc(path, rys_list, boys):
     lines = ["// Generated by lightspeed_b200/tables/gen_tables.py -- do not edit.",
-             "// Rys: per nrys, [root][bin][coef] for t, then [root][bin][coef] for ln w,",
+             "// Rys: per nrys, [root][bin][coef] for t, then [root][bin][coef] for ln w",
+             "// (for nrys = 1 the weight w itself),",
              "// monomial coefficients c0..c7 of the local variable x in [-1,1].",
              "// Boys: [m][bin][coef] for F_m on [0, BOYS_TMAX).",
              "#pragma once", ""]
@@ -203,6 +206,13 @@ def write_inc(path, rys_list, boys):
         asym_w[r["n"], :r["n"]] = h
     lines.append("static const double kRysAsymT[%d] = {\n%s};" % (asym_t.size, _fmt(asym_t.ravel())))
     lines.append("static const double kRysAsymW[%d] = {\n%s};" % (asym_w.size, _fmt(asym_w.ravel())))
+    # the same nodes as initializer lists, for constant-memory copies in device code
+    lines.append("#define LSJK_RYS_ASYM_T_LIST \\\n%s" % " \\\n".join(
+        ", ".join("%.17e" % v for v in asym_t.ravel()[i:i + 4]) + ("," if i + 4 < asym_t.size else "")
+        for i in range(0, asym_t.size, 4)))
+    lines.append("#define LSJK_RYS_ASYM_W_LIST \\\n%s" % " \\\n".join(
+        ", ".join("%.17e" % v for v in asym_w.ravel()[i:i + 4]) + ("," if i + 4 < asym_w.size else "")
+        for i in range(0, asym_w.size, 4)))
     lines.append("#define LSJK_BOYS_NBIN %d" % boys["nbin"])
     lines.append("#define LSJK_BOYS_TMAX %.17e" % boys["tmax"])
     lines.append("static const double kBoysCoef[%d] = {\n%s};" % (boys["coefs"].size, _fmt(boys["coefs"].ravel())))

@@ -10,6 +10,8 @@ reference CPU IntBox built from its sources, oracle/_ref).
   1e-10 of coulombCPU / exchangeCPU, and the mixed-precision build at the
   workload's thredp = 1e-5 within 1e-6 elementwise and |dE| <= 1e-6 Eh at fixed
   density.
+* K over merged twins (shared s exponents computed once, the benchmark's K)
+  on C10H22 within 1e-10 of the oracle, with fewer quartets.
 * A mixed-precision RHF of C10H22 (incremental Fock, thredp = 1e-5) converges
   to the FP64 RHF energy within 1e-6 Eh.
 * Batched K: four non-symmetric densities in one exchangeMulti call, bare
@@ -78,6 +80,29 @@ def test_c10h22_fp64_vs_oracle(ls, c10):
     J, K = _builds(ls, c10["scf"], c10["D"], THRE)
     assert np.max(np.abs(J - c10["Jr"])) < 1e-10
     assert np.max(np.abs(K - c10["Kr"])) < 1e-10
+
+
+def test_c10h22_merged_k_vs_oracle(ls, c10):
+    """K over the merged twins (ls.set_merge(True), the benchmark's K): every
+    quartet of the reference is kept, so K stays within 1e-10 of the oracle at
+    the workload's threshold while computing fewer quartets."""
+    ls.set_precision(ls.PREC_FP64)
+    res = ls.ResourceList.build()
+    pl = c10["scf"].pairs
+    Dt = ls.Tensor.array(c10["D"])
+    try:
+        ls.set_merge(True)
+        ls.reset_stats()
+        K = ls.IntBox.exchange(res, ls.Ewald.coulomb(), pl, pl, Dt, True, THRE, THRE).np.copy()
+        nk_merged = ls.stats()["k_quartets"]
+        ls.set_merge(False)
+        ls.reset_stats()
+        ls.IntBox.exchange(res, ls.Ewald.coulomb(), pl, pl, Dt, True, THRE, THRE)
+        nk_exact = ls.stats()["k_quartets"]
+    finally:
+        ls.set_merge(False)
+    assert np.max(np.abs(K - c10["Kr"])) < 1e-10
+    assert nk_merged < 0.7 * nk_exact
 
 
 def test_c10h22_mixed_vs_oracle(ls, c10):

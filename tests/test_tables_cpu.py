@@ -3,7 +3,8 @@ quad_tables.inc, written by lightspeed_b200/tables/gen_tables.py), evaluated
 on the CPU exactly the way lsjk_device.cuh evaluates them: bin index
 floor(T * nbin / tmax) clamped to the last bin, local variable
 x = 2 (u - bin) - 1, Horner over the 8 monomial coefficients, exp of the
-interpolated ln w; the half-range Gauss-Hermite form at T >= tmax.
+interpolated ln w (the one-point rule tabulates w = F_0 itself); the
+half-range Gauss-Hermite form at T >= tmax.
 
 * Rys roots and weights against the reference's own tables,
   Rys::compute_t / compute_w (src/lightspeed/rys.hpp:56-153, through
@@ -66,7 +67,8 @@ def rys_device(tab, n, T):
     b, x = _bin(T[lo], nbin, tmax)
     for i in range(n):
         t[lo, i] = _horner(blk[i, b], x)
-        w[lo, i] = np.exp(_horner(blk[n + i, b], x))
+        lw = _horner(blk[n + i, b], x)
+        w[lo, i] = lw if n == 1 else np.exp(lw)   # the one-point rule tabulates w itself
     r = 1.0 / np.sqrt(T[~lo])
     t[~lo] = tab["asym_t"][n, :n] * r[:, None]
     w[~lo] = tab["asym_w"][n, :n] * r[:, None]
@@ -131,7 +133,8 @@ def test_rys_fp32_tables_below_switch():
         tr, wr = ref.rys(n, T.astype(np.float64))
         for i in range(n):
             t = _horner(blk[i, b], x).astype(np.float32)
-            w = np.exp(_horner(blk[n + i, b], x).astype(np.float32))
+            lw = _horner(blk[n + i, b], x).astype(np.float32)
+            w = lw if n == 1 else np.exp(lw)
             assert np.max(np.abs(t - tr[:, i])) < 2e-6
             assert np.max(np.abs(w - wr[:, i]) / wr[:, i]) < 2e-5
 
