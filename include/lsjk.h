@@ -69,6 +69,11 @@ const char* lsjk_last_error(void);
 /* Library version string. */
 const char* lsjk_version(void);
 
+/* Number of device allocations (cudaMalloc) the library has made since it was
+ * loaded, over all contexts: a caller can check that a call allocated nothing
+ * by reading it before and after. No counterpart in the reference. */
+long lsjk_device_allocations(void);
+
 /* ---- context: one per device; owns the stream, tables and scratch memory.
  * Replaces the TCIntBox session (tc/tcintbox/tcintbox.cpp:20-50). */
 int lsjk_context_create(int device, lsjk_context** out);
@@ -192,8 +197,9 @@ int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, con
  * LSJK_NOALLOC_SCRATCH_BYTES that each GPU loading this library holds until
  * the process exits; a build that needs more is rejected with LSJK_ENOMEM
  * (and a message naming the limit) before anything is written to J12_dev.
- * The first call on a device looks up the array's device address (make that
- * first call before any stream capture). All calls on a device share the
+ * The first call on a device (and again after a device reset replaced its
+ * CUDA context) looks up the array's device address: make that first call
+ * before any stream capture. All calls on a device share the
  * array, which keeps the previous call's contents (the build clears what must
  * start at zero), so calls whose GPU work overlaps -- on different streams or
  * contexts of the same device -- race. */

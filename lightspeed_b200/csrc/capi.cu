@@ -1,6 +1,7 @@
 // extern "C" entry points of liblsjk.so (declared in include/lsjk.h).
 #include <algorithm>
 #include <cstring>
+#include <dlfcn.h>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -253,6 +254,8 @@ int lsjk_measure_fma_peak(lsjk_context* ctx, int fp64, double* tflops)
 }
 
 const char* lsjk_last_error(void) { return g_err.c_str(); }
+
+long lsjk_device_allocations(void) { return lsjk::g_device_allocations.load(std::memory_order_relaxed); }
 
 const char* lsjk_version(void) { return "lsjk 0.1 (sm_100a)"; }
 
@@ -765,26 +768,54 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[LSJK_NOALLOC_SC
 
 namespace {
 
-// Device address of g_noalloc_scratch, looked up once per device. In host
-// code the name g_noalloc_scratch is only a host-side stand-in for the device
-// object; a kernel given it would fault (or, where the GPU can reach host
-// memory, silently use the wrong memory), so kernels get this address.
+// The CUDA context current on this thread (the driver's cuCtxGetCurrent,
+// found in the driver library the runtime has already loaded), or null if
+// it cannot be read.
+void* current_cuda_context()
+{
+    using Fn = int (*)(void**);
+    static Fn fn = [] {
+        void* h = dlopen("libcuda.so.1", RTLD_LAZY | RTLD_NOLOAD);
+        return h ? reinterpret_cast<Fn>(dlsym(h, "cuCtxGetCurrent")) : nullptr;
+    }();
+    void* c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Device address of g_noalloc_scratch, looked up once per device and CUDA
+// context (a device reset makes a new context, and the address is looked up
+// again). In host code the name g_noalloc_scratch is only a host-side
+// stand-in for the device object; a kernel given it would fault (or, where
+// the GPU can reach host memory, silently use the wrong memory), so kernels
+// get this address.
 char* noalloc_scratch_address(int device)
 {
+    struct Entry {
+        int device;
+        void* context;
+        char* addr;
+    };
     static std::mutex mu;
-    static std::vector<char*> addr;
+    static std::vector<Entry> cache;
     std::lock_guard<std::mutex> lock(mu);
     if (device < 0) throw lsjk::Error(LSJK_EINVAL, "noalloc: bad device");
-    if ((int) addr.size() <= device) addr.resize(device + 1, nullptr);
-    if (!addr[device]) {
-        void* p = nullptr;
-        // the caller made `device` current (set_device)
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            throw lsjk::Error(LSJK_ECUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        addr[device] = static_cast<char*>(p);
-    }
-    return addr[device];
+    // the caller made `device` current (set_device), so its context is current too
+    void* context = current_cuda_context();
+    for (const Entry& e : cache)
+        if (e.device == device && e.context == context) return e.addr;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        throw lsjk::Error(LSJK_ECUDA, std::string("noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    for (Entry& x : cache)
+        if (x.device == device) {   // the device's earlier context is gone
+            x.context = context;
+            x.addr = static_cast<char*>(p);
+            return x.addr;
+        }
+    cache.push_back(Entry{device, context, static_cast<char*>(p)});
+    return static_cast<char*>(p);
 }
 
 // Points the context's scratch allocator at the static array for the lifetime
@@ -917,11 +948,12 @@ extern "C" int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, co
                           int sym34, int sym1234, float thresp, float thredp, double* I)
 {
     return guard([&] {
-        if (!ctx || !pl12 || !pl34) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        // the orbital counts are checked first: they need no device
         if (n1 < 0 || n2 < 0 || n3 < 0 || n4 < 0) throw lsjk::Error(LSJK_EINVAL, "negative orbital count");
         if ((sym12 && n1 != n2) || (sym34 && n3 != n4) || (sym1234 && (n1 != n3 || n2 != n4)))
             throw lsjk::Error(LSJK_EINVAL, "a symmetry flag needs equal orbital counts");
         if (n3 > 65535) throw lsjk::Error(LSJK_EINVAL, "lsjk_eri_j: at most 65535 orbitals in C3");
+        if (!ctx || !pl12 || !pl34) throw lsjk::Error(LSJK_EINVAL, "null argument");
         const size_t nI = (size_t) n1 * n2 * n3 * n4;
         if (nI && (!C1 || !C2 || !C3 || !C4 || !I)) throw lsjk::Error(LSJK_EINVAL, "null argument");
         lsjk::Context* c = &ctx->c;

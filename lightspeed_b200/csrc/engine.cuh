@@ -13,6 +13,7 @@
 //        CSR rows per (L_indexed, L_partner) class, with the partner data
 //        (K_ab prefactor, exponent, centre, cartIdx, bound) in SoA.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -48,6 +49,10 @@ struct Error : std::runtime_error {
                                                cudaGetErrorString(e_));                    \
     } while (0)
 
+// Device allocations the library has made since it was loaded (every
+// cudaMalloc goes through DBuf::alloc); read by lsjk_device_allocations().
+inline std::atomic<long> g_device_allocations{0};
+
 // Device buffer owned by RAII (freed with the context's stream-ordered pool).
 template <typename T>
 struct DBuf {
@@ -63,6 +68,7 @@ struct DBuf {
         release();
         n = count;
         if (count == 0) return;
+        g_device_allocations.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
         if (e != cudaSuccess) {
             p = nullptr;

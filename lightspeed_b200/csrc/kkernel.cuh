@@ -64,7 +64,8 @@ constexpr int kKGrab = 16;
 // warp as shared-memory broadcasts (64 bytes).
 struct alignas(16) KHdr {
     double dRx, dRy, dRz;   // R2 - R4 (pair data are relative to these centres)
-    int s12, n12, s34, n34; // K-invert rows of prim2 (partners 1) and prim4 (partners 3)
+    int s12, n12, s34, n34; // K-invert rows of prim2 (partners 1) and prim4 (partners 3; n34: the
+                            // prefix of the row that can pass the screens)
     int c2, c4;             // Cartesian offsets of prim2 and prim4
     float tlo, thi;         // float thresholds on bound12 * bound34 for this task's max|D24|
     float b12max;           // largest bound of the partner-1 row
@@ -272,6 +273,17 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
             h.tlo = float_threshold(thr_lo, T.dmax);
             h.thi = float_threshold(thr_hi, T.dmax);
             h.b12max = A.b12[h.s12];   // first segment's first entry: the row maximum
+            // partners 3 that can pass with the row's largest partner-1 bound: a prefix of
+            // the bound-ordered row (b34 >= thre34 and b12max * b34 >= tlo, both monotone)
+            {
+                int lo = 0, hi = h.n34;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    const float b = A.b34[h.s34 + mid];
+                    if (b >= thre34 && h.b12max * b >= h.tlo) lo = mid + 1; else hi = mid;
+                }
+                h.n34 = lo;
+            }
             // symmetric D24 (A.flip): the transposed contribution of a task with i2 != i4 is
             // not written here; the build adds K13 to its transpose afterwards, and tasks with
             // i2 == i4 (whose contribution is symmetric) enter with weight 1/2
@@ -279,13 +291,51 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
             hdr[lane] = h;
         }
         __syncwarp();
+        // Packs: the lanes of the warp take partners 3 of one or more consecutive tasks of
+        // the grab that share prim2 (hence the same partner-1 row), a lane each, so short
+        // partner-3 rows (p and d partners) and the tail of a long row fill the warp
+        // together; each lane keeps its own task's thresholds, D24 block and centres.
+        int pos = 0, koff = 0;
 #pragma unroll 1
-        for (int jt = 0; jt < nt; ++jt) {
-            const KHdr H = hdr[jt];
-            const double wsym = (double) H.wsym;
-            const float tlo = H.tlo, thi = H.thi;
-            const R dRx = (R) H.dRx, dRy = (R) H.dRy, dRz = (R) H.dRz;
-            const int c2 = H.c2, c4 = H.c4;
+        for (;;) {
+            while (pos < nt && hdr[pos].n34 == 0) ++pos;
+            if (pos >= nt) break;
+            const int s12 = hdr[pos].s12, n12 = hdr[pos].n12, c2 = hdr[pos].c2;
+            int my_task = -1, my_k = 0;
+            {
+                int filled = 0, at = pos, k0 = koff;
+                while (filled < 32 && at < nt && hdr[at].s12 == s12) {
+                    const int n = hdr[at].n34;
+                    const int len = min(n - k0, 32 - filled);
+                    if (lane >= filled && lane < filled + len) {
+                        my_task = at;
+                        my_k = k0 + lane - filled;
+                    }
+                    filled += len;
+                    k0 += len;
+                    if (k0 < n) break;   // this task goes on in the next pack
+                    ++at;
+                    k0 = 0;
+                }
+                pos = at;
+                koff = k0;
+            }
+            const bool in3 = my_task >= 0;
+            float tlo = __int_as_float(0x7f800000), thi = 0.0f;
+            double wsym = 1.0;
+            R dRx = 0, dRy = 0, dRz = 0;
+            int k3 = 0, c4 = 0;
+            if (in3) {
+                const KHdr& H = hdr[my_task];
+                tlo = H.tlo;
+                thi = H.thi;
+                wsym = (double) H.wsym;
+                dRx = (R) H.dRx;
+                dRy = (R) H.dRy;
+                dRz = (R) H.dRz;
+                k3 = H.s34 + my_k;
+                c4 = H.c4;
+            }
             R Dblk[NG][N2 * N4];
 #pragma unroll
             for (int g = 0; g < NG; ++g)
@@ -293,16 +343,9 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                 for (int a = 0; a < N2; ++a)
 #pragma unroll
                     for (int b = 0; b < N4; ++b)
-                        Dblk[g][a * N4 + b] = (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b];
-            const int s12 = H.s12, n12 = H.n12;
-            const int s34 = H.s34, n34 = H.n34;
-            const float b12_max = H.b12max;
-
-            for (int cs = 0; cs < n34; cs += 32) {
-                // partner 3 of this lane: entry cs + lane of the row
-                // (all loads of the entry issue together; the bound screen applies afterwards)
-                const int k3 = s34 + cs + lane;
-                const bool in3 = cs + lane < n34;
+                        Dblk[g][a * N4 + b] = in3 ? (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b] : R(0);
+            {
+                // partner 3 of this lane (all loads of the entry issue together)
                 float b34 = 0.0f;
                 R kab34 = 0, q = 1, iq = 1, Qx = 0, Qy = 0, Qz = 0, Cx = 0, Cy = 0, Cz = 0;
                 int c3 = 0, c3b = -1;
@@ -319,16 +362,11 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                         w31 = A.w1_34[k3];
                     }
                 }
-                const bool v3 = in3 && b34 >= thre34;
-                if (!v3) b34 = 0.0f;
+                // (every lane of a pack passes thre34 and the row's first partner 1)
+                const bool v3 = in3;
                 const R QCx = Qx - Cx, QCy = Qy - Cy, QCz = Qz - Cz;
                 // ket side of PQ: (Q - R4) with the task's centre shift folded in
                 const R Sx = dRx - Qx, Sy = dRy - Qy, Sz = dRz - Qz;
-                float bmax34 = b34;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) bmax34 = fmaxf(bmax34, __shfl_xor_sync(0xffffffffu, bmax34, o));
-                // partners 3 come by bound: no later chunk passes either
-                if (bmax34 == 0.0f || b12_max * bmax34 < tlo) break;
                 // segment accumulators: acc for the segment's first target, accb for its
                 // second (s-type partners 1 may stand for two contracted shells)
                 R acc[NG][N1 * N3];
@@ -400,25 +438,29 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                     for (int j = 0; j < kend; ++j) {
                         const float b12 = cur[j].b;
                         const int sg = cur[j].seg;
+                        // can this lane's quartet reach its lower threshold (or any later one of the
+                        // segment / of later segments, whose bounds are not larger)?
+                        const float est = b12 * b34;
+                        const bool can = v3 && est >= tlo;
+                        const bool any_can = b12 >= thre12 && __any_sync(0xffffffffu, can);
                         if (sg != prev_seg) {
                             flush();
                             prev_seg = sg;
                             prev_c1 = cur[j].c;
                             if constexpr (G1 == 2) prev_c1b = cur[j].t1;
                             // segments are ordered by their largest bound: nothing later passes
-                            if (b12 < thre12 || b12 * bmax34 < tlo) {
+                            if (!any_can) {
                                 stop = true;
                                 break;
                             }
-                        } else if (b12 < thre12 || b12 * bmax34 < tlo) {
+                        } else if (!any_can) {
                             // entries of a segment are ordered by bound: skip the rest of this
                             // segment within the chunk (to the next segment start, or the chunk end)
                             const unsigned nxt = j == 31 ? 0u : (chg & ~((2u << j) - 1u));
                             j = (nxt ? __ffs(nxt) - 1 : kend) - 1;
                             continue;
                         }
-                        const float est = b12 * b34;
-                        const bool pass = v3 && est >= tlo && est < thi;
+                        const bool pass = can && est < thi;
                         if (!__any_sync(0xffffffffu, pass)) continue;
                         if (!pass) continue;
                         const KEnt<R> e = cur[j];

@@ -70,3 +70,18 @@ def test_tensor_numpy_view(ls):
     v[1, 2] = -5.0
     assert t.np[1, 2] == -5.0
     assert np.asarray(t).shape == (3, 4)
+
+
+def test_eri_j_rejects_more_than_65535_c3_orbitals(ls):
+    """lsjk_eri_j's C3 count is the grid height of its left contraction kernel:
+    65536 orbitals are refused before any device work, with LSJK_EINVAL."""
+    lib = ctypes.CDLL(ls.LIB_PATH)
+    lib.lsjk_last_error.restype = ctypes.c_char_p
+    f = ctypes.c_float(1e-14)
+    rc = lib.lsjk_eri_j(None, 1, None, None, None, None, 1, 1, 65536, 1, None, None, None, None, 0, 0, 0, f, f,
+                        None)
+    assert rc == 1   # LSJK_EINVAL
+    assert b"65535" in lib.lsjk_last_error()
+    rc = lib.lsjk_eri_j(None, 1, None, None, None, None, 1, 1, 65535, 1, None, None, None, None, 0, 0, 0, f, f,
+                        None)
+    assert rc == 1 and b"null argument" in lib.lsjk_last_error()

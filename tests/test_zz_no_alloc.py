@@ -9,8 +9,12 @@ the C ABI (ctypes on liblsjk.so, device buffers from torch) and compare it
 with lsjk_coulomb_device on the same context, pair list and density, for two
 calls in a row (the static array keeps the previous call's contents, so the
 second call shows that nothing stale leaks in), at the 1e-10 elementwise
-tolerance of the other J/K parity tests. A basis too large for the array is
-rejected with LSJK_ENOMEM and a message, and leaves J unchanged.
+tolerance of the other J/K parity tests. The first of these calls is the
+first build on a fresh context, and the library's count of device
+allocations (lsjk_device_allocations) does not move over the two calls. A
+basis whose Cartesian D and J alone do not fit the array, and one whose D and
+J fit but whose whole build does not, are rejected with LSJK_ENOMEM and a
+message, leave J unchanged, and leave the context usable.
 
 This file is collected last on purpose."""
 import ctypes
@@ -27,6 +31,7 @@ LSJK_PREC_FP64 = 1
 def _lib(ls):
     lib = ctypes.CDLL(ls.LIB_PATH)
     lib.lsjk_last_error.restype = ctypes.c_char_p
+    lib.lsjk_device_allocations.restype = ctypes.c_long
     return lib
 
 
@@ -98,15 +103,21 @@ def test_noalloc_matches_device_entry_two_calls(ls):
     api = CApi(ls, bas, 1e-12)
     try:
         n = bas.nao
-        for call, seed in enumerate((1, 2)):
-            D = torch.tensor(_density(n, seed), device="cuda")
+        Ds = [torch.tensor(_density(n, seed), device="cuda") for seed in (1, 2)]
+        J_new = [torch.zeros((n, n), dtype=torch.float64, device="cuda") for _ in Ds]
+        api.sync()   # torch filled the buffers on its own stream
+        # the two no-alloc calls first: the first J build of this fresh context
+        allocs = api.lib.lsjk_device_allocations()
+        for D, J in zip(Ds, J_new):
+            api._ok(api.coulomb_noalloc(D, J, 1e-12))
+        api.sync()
+        assert api.lib.lsjk_device_allocations() == allocs, "a no-alloc call allocated device memory"
+        for call, (D, J) in enumerate(zip(Ds, J_new)):
             J_ref = torch.zeros((n, n), dtype=torch.float64, device="cuda")
-            J_new = torch.zeros((n, n), dtype=torch.float64, device="cuda")
-            api.sync()   # torch filled the buffers on its own stream
-            api._ok(api.coulomb_device(D, J_ref, 1e-12))
-            api._ok(api.coulomb_noalloc(D, J_new, 1e-12))
             api.sync()
-            diff = (J_new - J_ref).abs().max().item()
+            api._ok(api.coulomb_device(D, J_ref, 1e-12))
+            api.sync()
+            diff = (J - J_ref).abs().max().item()
             assert J_ref.abs().max().item() > 1e-3, "empty reference J"
             assert diff < 1e-10, "call %d: max |dJ| = %.3e" % (call + 1, diff)
     finally:
@@ -128,5 +139,35 @@ def test_noalloc_rejects_too_large(ls):
         assert rc == LSJK_ENOMEM
         assert b"static scratch" in api.lib.lsjk_last_error()
         assert bool((J == 7.0).all().item()), "a rejected call wrote to J"
+    finally:
+        api.close()
+
+
+def test_noalloc_rejects_a_build_that_outgrows_the_array(ls):
+    """D and J (2 x 1368^2 doubles, 30 MB) fit the 32 MiB array, the ket
+    records and sort space of the build do not: the build itself refuses,
+    before anything reaches J, and the context's own scratch is back in place
+    for the next ordinary call."""
+    import torch
+    from lightspeed_b200.geometry import water_cluster
+    bas = ls.Basis.from_gbs_file(water_cluster(72, seed=2), "6-31gs")
+    assert 2 * bas.ncart ** 2 * 8 < (32 << 20)
+    api = CApi(ls, bas, 1e-12)
+    try:
+        n = bas.nao
+        D = torch.tensor(_density(n, 4), device="cuda")
+        J = torch.full((n, n), 7.0, dtype=torch.float64, device="cuda")
+        api.sync()
+        rc = api.coulomb_noalloc(D, J, 1e-12)
+        api.sync()
+        assert rc == LSJK_ENOMEM
+        msg = api.lib.lsjk_last_error()
+        assert b"static scratch" in msg and b"this J build" in msg
+        assert bool((J == 7.0).all().item()), "a rejected call wrote to J"
+        J2 = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        api.sync()
+        api._ok(api.coulomb_device(D, J2, 1e-12))
+        api.sync()
+        assert J2.abs().max().item() > 1e-3
     finally:
         api.close()
