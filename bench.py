@@ -228,8 +228,23 @@ def run_ours(args):
     t0 = time.time()
     from lightspeed_b200.sad import SAD
     scf = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THRE)
-    E_scf = scf.compute(D0=SAD(ls, "cc-pvdz").density(mol, bas), maxiter=args.scf_maxiter, g_conv=1e-6)
+    D_sad = SAD(ls, "cc-pvdz").density(mol, bas)
+    E_scf = scf.compute(D0=D_sad, maxiter=args.scf_maxiter, g_conv=1e-6)
     t_scf = time.time() - t0
+    # the same SCF with mixed-precision J/K (quartets below thredp in FP32, incremental
+    # Fock builds on FP64 difference densities): energy error per iteration and at
+    # convergence against the FP64 SCF
+    scf_mixed = None
+    if not args.profile_step:
+        ls.set_precision(ls.PREC_MIXED)
+        t0 = time.time()
+        scf_mx = RHF(ls, mol, bas, thre_pq=THRE, thre_sp=THRE, thre_dp=THREDP)
+        E_mx = scf_mx.compute(D0=D_sad, maxiter=args.scf_maxiter, g_conv=1e-6)
+        n = min(len(scf.trace), len(scf_mx.trace))
+        scf_mixed = {"energy": E_mx, "dE_final_Eh": E_mx - E_scf, "converged": bool(scf_mx.converged),
+                     "iterations": len(scf_mx.trace), "seconds": time.time() - t0,
+                     "dE_per_iteration_Eh": [scf_mx.trace[k]["E"] - scf.trace[k]["E"] for k in range(n)]}
+        ls.set_precision(ls.PREC_FP64)
     D = scf.D
     pl = scf.pairs
     ew = ls.Ewald.coulomb()
@@ -402,7 +417,7 @@ def run_ours(args):
         "system": {"nao": nao, "ncart": bas.ncart, "nprim": bas.nprim,
                    "parallelism": "replicas" if world > 1 else "single-gpu", "scf_iterations": len(scf.trace),
                    "scf_energy": E_scf, "scf_converged": bool(scf.converged), "scf_guess": "SAD",
-                   "scf_seconds": t_scf},
+                   "scf_seconds": t_scf, "scf_mixed": scf_mixed},
         # K over merged twins (shared s exponents computed once; ls.set_merge): the same K up to
         # quartets below thresp (dE_merged_vs_exact_Eh at fixed density); "exact" is the same
         # step over the reference's exact quartet set

@@ -226,6 +226,17 @@ int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, const double*
                const double* C1, const double* C2, const double* C3, const double* C4, int sym12, int sym34,
                int sym1234, float thresp, float thredp, double* I);
 
+/* J nuclear gradient, replaces IntBox::coulombGrad (src/lightspeed/intbox.hpp:998-1008,
+ * src/cpp/intbox/intbox.cpp:423-491; CPU kernels src/cpp/intbox/cpu/coulomb_grad.cpp):
+ * G (natom x 3, row-major, host) += sum_{pqrs} D12_pq d(pq|rs)/dR D34_rs over a
+ * symmetric pair list; D12, D34 are host nao x nao matrices (the same pointer
+ * for D12 == D34, the reference's symmetric branch). FP64 throughout (thredp
+ * is ignored, as on the reference's CPU path); quartets screened like J
+ * (B_pq B_rs max|D34 block| >= thresp). LSJK_EINVAL for a non-symmetric list. */
+int lsjk_coulomb_grad(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                      const lsjk_pairlist* pl, const double* D12, const double* D34, float thresp, float thredp,
+                      double* G);
+
 /* ---- CUDA graphs: capture the builds issued through the *_device entry
  * points between lsjk_graph_begin and lsjk_graph_end on the context stream,
  * then replay them with one lsjk_graph_launch (an SCF iteration's J+K as one

@@ -65,7 +65,8 @@ def cuda_units():
     units = []
     for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "mlp"):
         units.append((name, os.path.join(CSRC, name + ".cu"), []))
-    for lb in range(2 * LMAX + 1):
+    # bra Hermite classes 0..2*LMAX, and 2*LMAX+1 for the gradients
+    for lb in range(2 * LMAX + 2):
         units.append(("jinst_%d" % lb, os.path.join(CSRC, "jinst.cu"), ["-DLSJK_LB=%d" % lb]))
     for l1 in range(LMAX + 1):
         for l2 in range(LMAX + 1):

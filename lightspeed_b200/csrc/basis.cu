@@ -120,6 +120,7 @@ void upload_prims(Context* ctx, Basis* B)
     B->dseg.upload(B->seg, s);
     B->dw0.upload(B->w0, s);
     B->dw1.upload(B->w1, s);
+    B->datom.upload(B->atom, s);
 }
 
 void upload_maps(Context* ctx, Basis* B, const std::vector<std::vector<std::pair<int, double>>>& c2p,

@@ -696,6 +696,41 @@ int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const doub
     });
 }
 
+int lsjk_coulomb_grad(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                      const lsjk_pairlist* pl, const double* D12, const double* D34, float thresp, float thredp,
+                      double* G)
+{
+    (void) thredp;   // FP64 throughout, as the reference's CPU gradient
+    return guard([&] {
+        if (!ctx || !pl || !D12 || !D34 || !G) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        const lsjk::PairList* p = &pl->p;
+        check_lmax(p);
+        if (!p->symm) throw lsjk::Error(LSJK_EINVAL, "IntBox::coulombGrad: pairlist must be symmetric");
+        const lsjk::Basis* b = p->b1;
+        const size_t nD = (size_t) b->nao * b->nao, nG = (size_t) b->natom * 3;
+        const bool same = D12 == D34;
+        c->scratch_reset();
+        double* dD = ctx->dev(2 * nD + nG);
+        double* dG = dD + 2 * nD;
+        double* h = ctx->io_host.ensure(2 * nD + nG);
+        std::memcpy(h, D12, sizeof(double) * nD);
+        std::memcpy(h + nD, D34, sizeof(double) * nD);
+        LSJK_CUDA(cudaMemcpyAsync(dD, h, sizeof(double) * 2 * nD, cudaMemcpyHostToDevice, c->stream));
+        LSJK_CUDA(cudaMemsetAsync(dG, 0, sizeof(double) * nG, c->stream));
+        double* D12c = lsjk::take<double>(c, (size_t) b->ncart * b->ncart);
+        double* D34c = same ? D12c : lsjk::take<double>(c, (size_t) b->ncart * b->ncart);
+        lsjk::pure_to_cart(c, b, b, dD, D12c);
+        if (!same) lsjk::pure_to_cart(c, b, b, dD + nD, D34c);
+        lsjk::coulomb_grad(c, ew, p, D12c, D34c, same, dG, thresp);
+        LSJK_CUDA(cudaMemcpyAsync(h, dG, sizeof(double) * nG, cudaMemcpyDeviceToHost, c->stream));
+        check_kernels(c);
+        for (size_t i = 0; i < nG; ++i) G[i] += h[i];
+    });
+}
+
 int lsjk_graph_begin(lsjk_context* ctx)
 {
     return guard([&] {

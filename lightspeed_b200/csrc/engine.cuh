@@ -97,6 +97,7 @@ struct BasisView {
     const int *L, *cart, *ao;
     const int *t0, *t1, *seg;
     const double *w0, *w1;
+    const int* atom;
 };
 
 struct Basis {
@@ -112,7 +113,7 @@ struct Basis {
     // device copies
     DBuf<double> dc, de, dx, dy, dz;
     DBuf<int> dL, dcart, dao;
-    DBuf<int> dt0, dt1, dseg;
+    DBuf<int> dt0, dt1, dseg, datom;
     DBuf<double> dw0, dw1;
     // pure <-> cart maps: cart row -> (pure index, coef) and pure row -> (cart index, coef)
     DBuf<int> c2p_off, c2p_idx, p2c_off, p2c_idx;
@@ -131,7 +132,7 @@ struct Basis {
     bool is_twin = false;   // this basis is a merged twin (some s primitives carry two targets)
     BasisView view() const {
         return BasisView{nprim, nao, ncart, dc.p, de.p, dx.p, dy.p, dz.p, dL.p, dcart.p, dao.p,
-                         dt0.p, dt1.p, dseg.p, dw0.p, dw1.p};
+                         dt0.p, dt1.p, dseg.p, dw0.p, dw1.p, datom.p};
     }
     bool equivalent(const Basis& o) const;
 };
@@ -322,6 +323,11 @@ constexpr int kJBatchMax = 4;
 // (screened with the largest |D| of the batch).
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                    const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp);
+// J nuclear gradient (FP64): G[atom][xyz] += sum D12 d(12|34) D34 over a symmetric
+// pair list, Cartesian densities in, device G (natom x 3) accumulated. `same`:
+// D12 and D34 are the same matrix (one bra-derivative pass, doubled).
+void coulomb_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D12cart, const double* D34cart,
+                  bool same, double* G, float thresp);
 // K for ng (1..4) densities sharing one task list (screened with the largest
 // |D24| of the batch) and the quartet integrals.
 // Dscr: the densities the screens read (Dcart itself when null, or screening

@@ -232,13 +232,14 @@ def main():
     os.makedirs(out_dir, exist_ok=True)
     head = ["// Generated by lightspeed_b200/csrc/gen_kernels.py -- do not edit.", "#pragma once",
             "#define LSJK_GEN_LMAX %d" % lmax, ""]
-    # J: Hermite classes 0..2*lmax
+    # J: Hermite classes 0..2*lmax, and bra classes one higher (2*lmax+1) for the
+    # nuclear gradients (the Hermite potential at a bra pair one order above its class)
     jparts = list(head)
-    for LB in range(2 * lmax + 1):
+    for LB in range(2 * lmax + 2):
         for LK in range(2 * lmax + 1):
             jparts.append(gen_j(LB, LK))
     jparts.append("template <int LB, int LK> struct JQ;")
-    for LB in range(2 * lmax + 1):
+    for LB in range(2 * lmax + 2):
         for LK in range(2 * lmax + 1):
             jparts.append("template <> struct JQ<%d, %d> { template <typename R> __device__ __forceinline__ static void "
                           "run(const R* a, R X, R Y, R Z, const R* dk, R* jp) { jq_B%d_K%d<R>(a, X, Y, Z, dk, jp); } };"

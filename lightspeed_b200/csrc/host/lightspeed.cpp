@@ -307,6 +307,25 @@ std::shared_ptr<Tensor> IntBox::coulomb(const std::shared_ptr<ResourceList>& res
                         J12 ? std::vector<std::shared_ptr<Tensor>>{J12} : std::vector<std::shared_ptr<Tensor>>{})[0];
 }
 
+std::shared_ptr<Tensor> IntBox::coulombGrad(const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ewald,
+                                            const std::shared_ptr<PairList>& pl, const std::shared_ptr<Tensor>& D12,
+                                            const std::shared_ptr<Tensor>& D34, float thresp, float thredp,
+                                            const std::shared_ptr<Tensor>& G)
+{
+    const size_t n = pl->basis1()->nao();
+    D12->shape_error({n, n});
+    D34->shape_error({n, n});
+    auto out = out_tensor(G, pl->basis1()->natom(), 3, "G");
+    // D12 == D34 (one object) is the reference's symmetric branch: pass one pointer
+    const double* d12 = D12->data().data();
+    const double* d34 = D12 == D34 ? d12 : D34->data().data();
+    check_rc(lsjk_coulomb_grad(Engine::instance().ctx(), (int) ewald->scales().size(), ewald->scales().data(),
+                               ewald->omegas().data(), pl->device_handle(), d12, d34, thresp, thredp,
+                               out->data().data()),
+             "IntBox::coulombGrad");
+    return out;
+}
+
 std::shared_ptr<Tensor> IntBox::exchange(const std::shared_ptr<ResourceList>& resources,
                                          const std::shared_ptr<Ewald>& ewald,
                                          const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,

@@ -206,6 +206,15 @@ public:
                                            const std::shared_ptr<PairList>& pairlist34,
                                            const std::shared_ptr<Tensor>& D34, float thresp, float thredp,
                                            const std::shared_ptr<Tensor>& J12 = std::shared_ptr<Tensor>());
+    // J nuclear gradient (src/lightspeed/intbox.hpp:998-1008): G (natom, 3) +=
+    // sum D12 d(12|34) D34 over a symmetric pair list; D12 and D34 the same
+    // object selects the symmetric branch, as in the reference.
+    static std::shared_ptr<Tensor> coulombGrad(const std::shared_ptr<ResourceList>& resources,
+                                               const std::shared_ptr<Ewald>& ewald,
+                                               const std::shared_ptr<PairList>& pairlist,
+                                               const std::shared_ptr<Tensor>& D12,
+                                               const std::shared_ptr<Tensor>& D34, float thresp, float thredp,
+                                               const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>());
     static std::shared_ptr<Tensor> exchange(const std::shared_ptr<ResourceList>& resources,
                                             const std::shared_ptr<Ewald>& ewald,
                                             const std::shared_ptr<PairList>& pairlist12,

@@ -164,6 +164,9 @@ PYBIND11_MODULE(_lightspeed, m)
         .def_static("coulomb", &IntBox::coulomb, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
                     py::arg("pairlist34"), py::arg("D34"), py::arg("thresp"), py::arg("thredp"),
                     py::arg("J12") = std::shared_ptr<Tensor>(), py::call_guard<py::gil_scoped_release>())
+        .def_static("coulombGrad", &IntBox::coulombGrad, py::arg("resources"), py::arg("ewald"), py::arg("pairlist"),
+                    py::arg("D12"), py::arg("D34"), py::arg("thresp"), py::arg("thredp"),
+                    py::arg("G") = std::shared_ptr<Tensor>(), py::call_guard<py::gil_scoped_release>())
         .def_static("exchange", &IntBox::exchange, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
                     py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"), py::arg("thresp"),
                     py::arg("thredp"), py::arg("K13") = std::shared_ptr<Tensor>(),

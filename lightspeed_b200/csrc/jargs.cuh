@@ -26,7 +26,9 @@ struct JArgs {
     int mixed;                // 1: quartets with estimate < thredp run in FP32
     float thredp;
     int chunk;                // ket pairs per CTA (grid.y = ceil(nket / chunk))
-    int ng;                   // densities in this launch (1..kJBatch); ket records hold ng blocks
+    int ng;                   // densities of the build (1..kJBatch)
+    int slots;                // density blocks per ket record (1, or kJBatch for a batched build)
+    int g0;                   // first density of this launch (a launch covers g0 .. g0 + NG - 1)
     long jbra_stride;         // distance between the densities' bra accumulators
     int nterm;
     double alpha[4], omega[4];

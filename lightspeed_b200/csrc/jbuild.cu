@@ -218,12 +218,12 @@ __global__ void k_ket_bounds(const unsigned* __restrict__ keys_sorted, const int
 // Hermite index t -> (tx, ty, tz) as a compile-time table (so unrolled loops
 // index registers, not memory).
 struct HermTab {
-    int x[35], y[35], z[35];
+    int x[56], y[56], z[56];   // Hermite orders up to 5 (the gradients' bra classes)
 };
 __host__ __device__ constexpr HermTab make_herm_tab()
 {
     HermTab T{};
-    for (int t = 0; t < 35; ++t) {
+    for (int t = 0; t < 56; ++t) {
         T.x[t] = herm_tx(t);
         T.y[t] = herm_ty(t);
         T.z[t] = herm_tz(t);
@@ -402,6 +402,99 @@ void launch_j_row(Context* ctx, const JArgs& A, int LK, int nbra_full, int nket_
 
 } // namespace
 
+// ---- J nuclear gradient: bra derivatives ---------------------------------------
+//
+// With the Hermite potential V_t of the ket density at a bra pair one order
+// above the pair's class (the J kernel run with bra class L1+L2+1), every
+// Cartesian integral of the pair and of its shifted partners is
+// pre * sum_t E^{ij}_t V_t. The derivative of a primitive Gaussian,
+//   d/dA_x phi_i = 2 alpha phi_{i+1x} - i_x phi_{i-1x},
+// then gives the pair's share of dE/dA and dE/dB, E = sum D_bra (ij|ket):
+//   dE/dA_x = pre sum_ij D_ij (2 alpha (i+1x, j|) - i_x (i-1x, j|)), and in j for B.
+template <int L1, int L2>
+__device__ void bra_grad(int i, int j, BasisView b1, BasisView b2, bool symm, const double* __restrict__ geom,
+                         const double* __restrict__ vt, const double* __restrict__ Dc, double scale,
+                         double* __restrict__ G)
+{
+    constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), H = nherm_of(L1 + L2 + 1);
+    constexpr HermTab ht = make_herm_tab();
+    constexpr CartTab ct = make_cart_tab();
+    const double p = geom[0];
+    const double P[3] = {geom[1], geom[2], geom[3]};
+    const double A[3] = {b1.x[i], b1.y[i], b1.z[i]};
+    const double B[3] = {b2.x[j], b2.y[j], b2.z[j]};
+    double PA[3], PB[3];
+    double R2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        PA[d] = P[d] - A[d];
+        PB[d] = P[d] - B[d];
+        R2 += (A[d] - B[d]) * (A[d] - B[d]);
+    }
+    const double e1 = b1.e[i], e2 = b2.e[j];
+    double pre = scale * kTwoPi52 / p * b1.c[i] * b2.c[j] * exp(-e1 * e2 / p * R2);
+    if (symm && i == j) pre *= 0.5;
+    ECoef<L1 + 1, L2 + 1> E;
+    build_E<L1 + 1, L2 + 1>(p, PA, PB, E);
+    auto I = [&](int lx, int ly, int lz, int mx, int my, int mz) {
+        double s = 0.0;
+#pragma unroll
+        for (int t = 0; t < H; ++t)
+            s += E.v[0][lx][mx][ht.x[t]] * E.v[1][ly][my][ht.y[t]] * E.v[2][lz][mz][ht.z[t]] * vt[t];
+        return s;
+    };
+    const int a1 = b1.cart[i], a2 = b2.cart[j], ld = b2.ncart;
+    double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int x = 0; x < N1; ++x)
+#pragma unroll 1
+        for (int y = 0; y < N2; ++y) {
+            double dxy = Dc[(long) (a1 + x) * ld + a2 + y];
+            if (symm) dxy += Dc[(long) (a2 + y) * ld + a1 + x];
+            if (dxy == 0.0) continue;
+            const int l[3] = {ct.x[L1][x], ct.y[L1][x], ct.z[L1][x]};
+            const int m[3] = {ct.x[L2][y], ct.y[L2][y], ct.z[L2][y]};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int ux = d == 0, uy = d == 1, uz = d == 2;
+                double ga = 2.0 * e1 * I(l[0] + ux, l[1] + uy, l[2] + uz, m[0], m[1], m[2]);
+                if (l[d] > 0) ga -= l[d] * I(l[0] - ux, l[1] - uy, l[2] - uz, m[0], m[1], m[2]);
+                double gb = 2.0 * e2 * I(l[0], l[1], l[2], m[0] + ux, m[1] + uy, m[2] + uz);
+                if (m[d] > 0) gb -= m[d] * I(l[0], l[1], l[2], m[0] - ux, m[1] - uy, m[2] - uz);
+                gA[d] += dxy * ga;
+                gB[d] += dxy * gb;
+            }
+        }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        atomicAdd(&G[3 * b1.atom[i] + d], pre * gA[d]);
+        atomicAdd(&G[3 * b2.atom[j] + d], pre * gB[d]);
+    }
+}
+
+template <int LB>
+__global__ void k_bra_grad(const int* __restrict__ nbra, const int* __restrict__ p1, const int* __restrict__ p2,
+                           const double* __restrict__ geom, BasisView b1, BasisView b2, int symm,
+                           const double* __restrict__ vbra, const double* __restrict__ Dc, double scale,
+                           double* __restrict__ G)
+{
+    constexpr int H = nherm_of(LB + 1);
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= *nbra) return;
+    int i = p1[k], j = p2[k];
+    int L1 = b1.L[i];
+    const double* g = geom + 4L * k;
+    const double* vt = vbra + (long) k * H;
+    if (LB == 0) bra_grad<0, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+    else if (LB == 1) { if (L1 == 1) bra_grad<1, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G); else bra_grad<0, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G); }
+    else if (LB == 2) {
+        if (L1 == 2) bra_grad<2, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+        else if (L1 == 1) bra_grad<1, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+        else bra_grad<0, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+    } else if (LB == 3) { if (L1 == 2) bra_grad<2, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G); else bra_grad<1, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G); }
+    else bra_grad<2, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+}
+
 // Algorithmic FP64/FP32 flops of one J quartet of Hermite class (LB|LK):
 // prefactor/geometry 16, Boys (table 8 FMA + L recursion steps + exp),
 // Hermite recursion (one FMA per R^{(n)}_{tuv}) and the contraction (2 flops
@@ -414,30 +507,33 @@ double j_quartet_flops(int LB, int LK)
     return 16.0 + (16.0 + 3.0 * L + 1.0) + 2.0 * nR + 2.0 * nherm_of(LB) * nherm_of(LK);
 }
 
-void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
-                   const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp)
+namespace {
+
+// Ket side of a J build and the bra truncation (stages 1 and 2), shared by the
+// J build and the J gradient: per ket Hermite class the screened, bound-sorted
+// ket records, and the device counts of kets and of bras that can pass.
+struct KetSet {
+    int* nket = nullptr;              // [kNHerm] kets kept per class (device)
+    int* nbra = nullptr;              // [kNHerm] bra pairs that can pass per class (device)
+    double* krec[kNHerm] = {};
+    float* krec32[kNHerm] = {};
+    float* kbound[kNHerm] = {};
+};
+
+KetSet prepare_kets(Context* ctx, const PairList* pl12, const PairList* pl34, const DSet& DS, float thresp,
+                    bool mixed)
 {
-    if (ng < 1 || ng > kJBatch) throw Error(LSJK_EINVAL, "coulomb_build: 1..4 densities per launch");
-    DSet DS{};
-    for (int g = 0; g < ng; ++g) DS.d[g] = Dcart[g];
-    DS.n = ng;
-    DS.slots = ng == 1 ? 1 : kJBatch;
     cudaStream_t s = ctx->stream;
-    const Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
+    const Basis *b3 = pl34->b1, *b4 = pl34->b2;
     // thresp / max12 (truncate_ket threshold), float as in the reference call
     const float thre_ket = (float) ((double) thresp / pl12->max_bound);
     int* counts = take<int>(ctx, 4 * kNHerm);          // nket[5], nbra[5]
     unsigned* maxbits = take<unsigned>(ctx, kNHerm);
-    unsigned long long* qcnt = ctx->counters.p;                          // FP64 J classes
-    unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass;  // FP32 J classes
     LSJK_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * 4 * kNHerm, s));
     LSJK_CUDA(cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * kNHerm, s));
-    int* nket = counts;
-    int* nbra = counts + kNHerm;
-    double* krec[kNHerm] = {};
-    float* krec32[kNHerm] = {};
-    float* kbound[kNHerm] = {};
-    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
+    KetSet K;
+    K.nket = counts;
+    K.nbra = counts + kNHerm;
 
     // 1. ket screening + sort per Hermite class
     for (int LK = 0; LK < kNHerm; ++LK) {
@@ -449,38 +545,63 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
         int* val = take<int>(ctx, n);
         int* perm = take<int>(ctx, n);
         k_ket_screen<<<nblk(n, 256), 256, 0, s>>>(jk.p1.p, jk.p2.p, jk.bound.p, n, b3->view(), b4->view(),
-                                                 pl34->symm ? 1 : 0, DS, thre_ket, key, val, nket + LK,
+                                                 pl34->symm ? 1 : 0, DS, thre_ket, key, val, K.nket + LK,
                                                  maxbits + LK);
         size_t tmp = 0;
         LSJK_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, key, keys, val, perm, n, 0, 32, s));
         void* t = ctx->scratch_take(tmp);
         LSJK_CUDA(cub::DeviceRadixSort::SortPairs(t, tmp, key, keys, val, perm, n, 0, 32, s));
-        krec[LK] = take<double>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
-        if (mixed) krec32[LK] = take<float>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
-        kbound[LK] = take<float>(ctx, n);
-        k_ket_bounds<<<nblk(n, 256), 256, 0, s>>>(keys, nket + LK, kbound[LK]);
+        double*& krec = K.krec[LK];
+        float*& krec32 = K.krec32[LK];
+        krec = take<double>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
+        if (mixed) krec32 = take<float>(ctx, (long) n * (4 + DS.slots * nherm_of(LK)));
+        K.kbound[LK] = take<float>(ctx, n);
+        k_ket_bounds<<<nblk(n, 256), 256, 0, s>>>(keys, K.nket + LK, K.kbound[LK]);
+        int* nk = K.nket + LK;
         switch (LK) {
-        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
-        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
-        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
-        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
-        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nket + LK, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec[LK], krec32[LK]); break;
+        case 0: k_ket_herm<0><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 1: k_ket_herm<1><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
         }
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches += 7;
     }
 
     // 2. bra truncation counts
-    {
-        BraTables T{};
-        for (int c = 0; c < kNHerm; ++c) {
-            T.bound[c] = pl12->jb[c].bound.p;
-            T.n[c] = pl12->jb[c].n;
-        }
-        k_bra_count<<<1, 32, 0, s>>>(maxbits, thresp, T, nbra);
-        LSJK_CUDA(cudaGetLastError());
-        ctx->stats.kernel_launches++;
+    BraTables T{};
+    for (int c = 0; c < kNHerm; ++c) {
+        T.bound[c] = pl12->jb[c].bound.p;
+        T.n[c] = pl12->jb[c].n;
     }
+    k_bra_count<<<1, 32, 0, s>>>(maxbits, thresp, T, K.nbra);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+    return K;
+}
+
+} // namespace
+
+void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
+                   const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp)
+{
+    if (ng < 1 || ng > kJBatch) throw Error(LSJK_EINVAL, "coulomb_build: 1..4 densities per launch");
+    DSet DS{};
+    for (int g = 0; g < ng; ++g) DS.d[g] = Dcart[g];
+    DS.n = ng;
+    DS.slots = ng == 1 ? 1 : kJBatch;
+    cudaStream_t s = ctx->stream;
+    const Basis *b1 = pl12->b1, *b2 = pl12->b2;
+    unsigned long long* qcnt = ctx->counters.p;                          // FP64 J classes
+    unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass;  // FP32 J classes
+    const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
+    const KetSet KS = prepare_kets(ctx, pl12, pl34, DS, thresp, mixed);
+    const int* nket = KS.nket;
+    int* nbra = KS.nbra;
+    double* const* krec = KS.krec;
+    float* const* krec32 = KS.krec32;
+    float* const* kbound = KS.kbound;
 
     // 3./4. J kernels
     double* jbra[kNHerm] = {};
@@ -528,6 +649,8 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
                 A.chunk = chunk;
             }
             A.ng = ng;
+            A.slots = DS.slots;
+            A.g0 = 0;
             A.jbra_stride = (long) jb.n * nherm_of(LB);
             A.nterm = (int) ew.alpha.size();
             for (int t = 0; t < A.nterm; ++t) {
@@ -595,6 +718,93 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             LSJK_CUDA(cudaGetLastError());
             ctx->stats.kernel_launches++;
         }
+}
+
+// One bra-derivative pass of the J gradient: kets from Dket, bra pairs
+// contracted with Dbra, derivatives at the bra centres into G.
+static void coulomb_grad_bra(Context* ctx, const Ewald& ew, const PairList* pl, const double* Dbra,
+                             const double* Dket, double scale, double* G, float thresp)
+{
+    cudaStream_t s = ctx->stream;
+    DSet DS{};
+    DS.d[0] = Dket;
+    DS.n = 1;
+    DS.slots = 1;
+    const KetSet KS = prepare_kets(ctx, pl, pl, DS, thresp, false);
+    for (int LB = 0; LB < kNHerm; ++LB) {
+        const JBraClass& jb = pl->jb[LB];
+        if (!jb.n) continue;
+        const int H1 = nherm_of(LB + 1);
+        double* vbra = take<double>(ctx, (long) jb.n * H1);
+        LSJK_CUDA(cudaMemsetAsync(vbra, 0, sizeof(double) * jb.n * H1, s));
+        for (int LK = 0; LK < kNHerm; ++LK) {
+            const JBraClass& jk = pl->jb[LK];
+            if (!jk.n) continue;
+            // the J kernel of bra class LB + 1 over the class-LB pairs: the Hermite potential
+            // of the ket density one order above the pairs' own class
+            JArgs A{};
+            A.bgeom = jb.geom.p;
+            A.bbound = jb.bound.p;
+            A.nbra = KS.nbra + LB;
+            A.jbra = vbra;
+            A.krec = KS.krec[LK];
+            A.kbound = KS.kbound[LK];
+            A.nket = KS.nket + LK;
+            A.boys = ctx->boys64.p + (long) (LB + 1 + LK) * LSJK_BOYS_NBIN * 8;
+            A.status = ctx->status.p;
+            A.qcount = A.qcount32 = ctx->tune_sink.p;
+            A.mixed = 0;
+            A.thredp = thresp;
+            int chunk = kJChunk;
+            const long tiles = (jb.n + kJThreads - 1) / kJThreads;
+            while (chunk > 64 && tiles * ((jk.n + chunk - 1) / chunk) < 2L * ctx->nsm) chunk >>= 1;
+            A.chunk = chunk;
+            A.ng = 1;
+            A.slots = 1;
+            A.g0 = 0;
+            A.jbra_stride = (long) jb.n * H1;
+            A.nterm = (int) ew.alpha.size();
+            for (int t = 0; t < A.nterm; ++t) {
+                A.alpha[t] = ew.alpha[t];
+                A.omega[t] = ew.omega[t];
+            }
+            A.thresp = thresp;
+            switch (LB + 1) {
+            case 1: launch_j_row<1>(ctx, A, LK, jb.n, jk.n); break;
+            case 2: launch_j_row<2>(ctx, A, LK, jb.n, jk.n); break;
+            case 3: launch_j_row<3>(ctx, A, LK, jb.n, jk.n); break;
+            case 4: launch_j_row<4>(ctx, A, LK, jb.n, jk.n); break;
+            case 5: launch_j_row<5>(ctx, A, LK, jb.n, jk.n); break;
+            }
+        }
+        const BasisView v1 = pl->b1->view(), v2 = pl->b2->view();
+        const unsigned gr = nblk(jb.n, 64);
+        switch (LB) {
+        case 0: k_bra_grad<0><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 1: k_bra_grad<1><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 2: k_bra_grad<2><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 3: k_bra_grad<3><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 4: k_bra_grad<4><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        }
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    }
+}
+
+// E = sum D12 (12|34) D34 moves with all four centres: its gradient is the
+// bra-centre derivative with D12 on the bra and D34 on the ket, plus the same
+// with the roles exchanged ((12|34) = (34|12)).
+void coulomb_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D12cart, const double* D34cart,
+                  bool same, double* G, float thresp)
+{
+    if (!pl->symm) throw Error(LSJK_EINVAL, "IntBox::coulombGrad: pairlist must be symmetric");
+    if (ew.alpha.empty() || !pl->npair) return;
+    if (same) {
+        coulomb_grad_bra(ctx, ew, pl, D12cart, D34cart, 2.0, G, thresp);   // both halves are this pass
+    } else {
+        coulomb_grad_bra(ctx, ew, pl, D12cart, D34cart, 1.0, G, thresp);
+        coulomb_grad_bra(ctx, ew, pl, D34cart, D12cart, 1.0, G, thresp);
+    }
 }
 
 } // namespace lsjk

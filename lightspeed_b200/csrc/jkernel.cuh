@@ -44,9 +44,16 @@ __device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, d
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g)
-            if (g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r + 4 + g * HK, jp[g]);
+            if (A.g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r + 4 + (A.g0 + g) * HK, jp[g]);
     }
 }
+
+// Densities of one J launch for a bra class: the batched kernel keeps NG x HB
+// FP64 accumulators per thread (and as many FP32 ones), so the heavy bra
+// classes take fewer densities per launch (more launches over the same ket
+// records) instead of spilling.
+template <int LB>
+__host__ __device__ constexpr int j_batch() { return nherm_of(LB) <= 4 ? kJBatch : (nherm_of(LB) <= 10 ? 2 : 1); }
 
 // Start of the last bin of the Boys table: from here on (the bin next to the
 // switch to the asymptotic form, and the asymptotic region itself) the FP32
@@ -99,7 +106,7 @@ __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, fl
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g)
-            if (g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4 + g * HK, jq[g]);
+            if (A.g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4 + (A.g0 + g) * HK, jq[g]);
     }
 #pragma unroll
     for (int g = 0; g < NG; ++g)
@@ -110,7 +117,8 @@ __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, fl
 template <int LB, int LK, int NG>
 __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 {
-    constexpr int HB = nherm_of(LB), S = 4 + NG * nherm_of(LK);
+    constexpr int HB = nherm_of(LB), HK = nherm_of(LK);
+    const int S = 4 + A.slots * HK;              // doubles (floats) per ket record
     __shared__ __align__(128) double tab[LSJK_BOYS_NBIN * 8];
     __shared__ __align__(128) float tab32[LSJK_BOYS_NBIN * 8];
     __shared__ __align__(8) uint64_t mbar[2];
@@ -168,8 +176,10 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 #pragma unroll
         for (int g = 0; g < NG; ++g)
 #pragma unroll
-            for (int t = 0; t < HB; ++t)
-                if (jp[g][t] != 0.0) atomicAdd(&A.jbra[g * A.jbra_stride + (long) i * HB + t], jp[g][t]);
+            for (int t = 0; t < HB; ++t) {
+                const double v = jp[g][t];
+                if (v != 0.0 && A.g0 + g < A.ng) atomicAdd(&A.jbra[(A.g0 + g) * A.jbra_stride + (long) i * HB + t], v);
+            }
     }
     // quartet counts for the statistics
     for (int o = 16; o > 0; o >>= 1) {
@@ -187,12 +197,21 @@ void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full)
 {
     if (nbra_full == 0 || nket_full == 0) return;
     dim3 grid((nbra_full + kJThreads - 1) / kJThreads, (nket_full + A.chunk - 1) / A.chunk);
-    if (A.ng <= 1)
-        k_coulomb<LB, LK, 1><<<grid, kJThreads, 0, ctx->stream>>>(A);
-    else
-        k_coulomb<LB, LK, kJBatch><<<grid, kJThreads, 0, ctx->stream>>>(A);
-    LSJK_CUDA(cudaGetLastError());
-    ctx->stats.kernel_launches++;
+    constexpr int NGB = j_batch<LB>();
+    // densities g0 .. g0 + NG - 1 per launch, over the same ket records
+    for (int g0 = 0; g0 < A.ng;) {
+        JArgs B = A;
+        B.g0 = g0;
+        if (A.ng - g0 >= NGB && NGB > 1) {
+            k_coulomb<LB, LK, NGB><<<grid, kJThreads, 0, ctx->stream>>>(B);
+            g0 += NGB;
+        } else {
+            k_coulomb<LB, LK, 1><<<grid, kJThreads, 0, ctx->stream>>>(B);
+            g0 += 1;
+        }
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    }
 }
 
 

@@ -139,6 +139,34 @@ def potential(pl, xyzZ, scales=(1.0,), omegas=(-1.0,), nthread=0):
     return out
 
 
+def coulomb_grad(pl, D12, D34=None, thresp=1e-14, thredp=1e-14, scales=(1.0,), omegas=(-1.0,), G=None,
+                 nthread=0):
+    """IntBox::coulombGrad: G (natom x 3) += sum D12 d(12|34) D34 (D34 None: the
+    same matrix, the reference's D12 == D34 branch)."""
+    s, o = _ewald(scales, omegas)
+    A = np.ascontiguousarray(D12, np.float64)
+    B = A if D34 is None else np.ascontiguousarray(D34, np.float64)
+    natom = int(pl.b1.arrs["atom"][-1]) + 1
+    out = np.zeros((natom, 3)) if G is None else np.array(G, np.float64, copy=True)
+    _check(lib().ref_coulomb_grad(pl.h, len(s), _p(s), _p(o), _p(A), _p(B), int(D34 is None), ctypes.c_float(thresp),
+                                  ctypes.c_float(thredp), _p(out), nthread))
+    return out
+
+
+def exchange_grad(pl, D13, D24=None, D13symm=True, D24symm=True, thresp=1e-14, thredp=1e-14, scales=(1.0,),
+                  omegas=(-1.0,), G=None, nthread=0):
+    """IntBox::exchangeGrad: G (natom x 3) += sum D13 d(12|34) D24 (D24 None: the
+    same matrix, Dsame)."""
+    s, o = _ewald(scales, omegas)
+    A = np.ascontiguousarray(D13, np.float64)
+    B = A if D24 is None else np.ascontiguousarray(D24, np.float64)
+    natom = int(pl.b1.arrs["atom"][-1]) + 1
+    out = np.zeros((natom, 3)) if G is None else np.array(G, np.float64, copy=True)
+    _check(lib().ref_exchange_grad(pl.h, len(s), _p(s), _p(o), _p(A), _p(B), int(D13symm), int(D24symm),
+                                   int(D24 is None), ctypes.c_float(thresp), ctypes.c_float(thredp), _p(out), nthread))
+    return out
+
+
 def rys(nrys, T):
     T = np.ascontiguousarray(T, np.float64)
     t = np.zeros((len(T), nrys))

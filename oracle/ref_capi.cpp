@@ -6,6 +6,9 @@
 // Reference entry points wrapped here (paths inside the reference project):
 //   IntBox::coulombCPU   src/cpp/intbox/cpu/coulomb.cpp:14-196
 //   IntBox::exchangeCPU  src/cpp/intbox/cpu/exchange.cpp:17-355
+//   IntBox::coulombGrad / exchangeGrad dispatch  src/cpp/intbox/intbox.cpp:423-630, restated
+//     over the CPU routines it selects (coulombGradSymmCPU / coulombGradAdvCPU,
+//     exchangeGradSymmCPU / exchangeGradAdvCPU in src/cpp/intbox/cpu/*_grad.cpp)
 //   PairList::build_schwarz src/cpp/core/pair_list.cpp:29-177
 //   IntBox::overlapCPU / kineticCPU / potentialCPU  src/cpp/intbox/cpu/*.cpp
 //   Rys::compute_t / compute_w  src/cpp/quad/rys.cpp:28-80
@@ -21,14 +24,14 @@
 #include <string>
 #include <vector>
 #include <exception>
+#include "ref_handles.hpp"
 
 using namespace lightspeed;
+using oracle_ref::RefBasis;
+using oracle_ref::RefPairs;
 
 namespace {
 thread_local std::string g_err;
-
-struct RefBasis { std::shared_ptr<Basis> b; };
-struct RefPairs { std::shared_ptr<PairList> p; };
 
 std::shared_ptr<ResourceList> resources(int nthread)
 {
@@ -140,6 +143,59 @@ int ref_exchange(void* pl12, void* pl34, int nterm, const double* scales, const 
         auto R = IntBox::exchangeCPU(resources(nthread), ew, p12, p34, D, D24symm != 0,
                                      thresp, thredp, K);
         std::memcpy(K13, R->data().data(), sizeof(double) * n1 * n3);
+        return 0;
+    } catch (std::exception& ex) { g_err = ex.what(); return 1; }
+}
+
+// G (natom x 3) += the J gradient sum D12 d(12|34) D34 (IntBox::coulombGrad;
+// `same` stands for the reference's test D12 == D34, an object identity).
+int ref_coulomb_grad(void* pl, int nterm, const double* scales, const double* omegas, const double* D12,
+                     const double* D34, int same, float thresp, float thredp, double* G, int nthread)
+{
+    try {
+        auto p = static_cast<RefPairs*>(pl)->p;
+        auto ew = std::make_shared<Ewald>(std::vector<double>(scales, scales + nterm),
+                                          std::vector<double>(omegas, omegas + nterm));
+        size_t n = p->basis1()->nao(), natom = p->basis1()->natom();
+        auto A = wrap(D12, n, n);
+        auto B = same ? A : wrap(D34, n, n);
+        auto Gt = wrap(G, natom, 3);
+        if (same) {
+            Gt = IntBox::coulombGradSymmCPU(resources(nthread), ew, p, A, thresp, thredp, Gt);
+        } else {
+            auto parts = IntBox::coulombGradAdvCPU(resources(nthread), ew, p, p, A, B, thresp, thredp,
+                                                   std::vector<std::shared_ptr<Tensor>>());
+            for (auto& t : parts)
+                for (size_t i = 0; i < Gt->size(); ++i) Gt->data()[i] += t->data()[i];
+        }
+        std::memcpy(G, Gt->data().data(), sizeof(double) * natom * 3);
+        return 0;
+    } catch (std::exception& ex) { g_err = ex.what(); return 1; }
+}
+
+// G (natom x 3) += the K gradient sum D13 d(12|34) D24 (IntBox::exchangeGrad).
+int ref_exchange_grad(void* pl, int nterm, const double* scales, const double* omegas, const double* D13,
+                      const double* D24, int D13symm, int D24symm, int Dsame, float thresp, float thredp,
+                      double* G, int nthread)
+{
+    try {
+        auto p = static_cast<RefPairs*>(pl)->p;
+        auto ew = std::make_shared<Ewald>(std::vector<double>(scales, scales + nterm),
+                                          std::vector<double>(omegas, omegas + nterm));
+        size_t n = p->basis1()->nao(), natom = p->basis1()->natom();
+        auto A = wrap(D13, n, n);
+        auto B = Dsame ? A : wrap(D24, n, n);
+        auto Gt = wrap(G, natom, 3);
+        if (D13symm && D24symm && Dsame) {
+            Gt = IntBox::exchangeGradSymmCPU(resources(nthread), ew, p, A, thresp, thredp, Gt);
+        } else {
+            auto parts = IntBox::exchangeGradAdvCPU(resources(nthread), ew, p, p, A, B, D13symm != 0,
+                                                    D24symm != 0, Dsame != 0, thresp, thredp,
+                                                    std::vector<std::shared_ptr<Tensor>>());
+            for (auto& t : parts)
+                for (size_t i = 0; i < Gt->size(); ++i) Gt->data()[i] += t->data()[i];
+        }
+        std::memcpy(G, Gt->data().data(), sizeof(double) * natom * 3);
         return 0;
     } catch (std::exception& ex) { g_err = ex.what(); return 1; }
 }

@@ -4,7 +4,8 @@ reference tree and oracle/_ref built; the fixtures are committed).
 1. ref_<case>.npz: the reference's own known-answer vectors for the J/K path,
    copied from its test data (tests/coverage/data/{prop,ewald,mix}_*.npz,
    checked by tests/coverage/prop_int.py:68-108, ewald_int.py:33-108 and
-   mix_basis.py:101-225 in the reference) -- only the density/J/K keys.
+   mix_basis.py:101-225 in the reference) -- only the density/J/K keys and
+   the J/K nuclear gradients (Jgr..Jgr4, Kgr..Kgr4 of prop_int.py:142-214).
 2. oracle_w8.npz: J and K of the reference CPU IntBox (oracle/_ref) for an
    8-water 6-31G* cluster (seed 0) at thresp = 1e-12 with the density
    D = C C^T of 40 seeded Gaussian columns Loewdin-orthonormalised in the
@@ -27,7 +28,8 @@ def copy_reference_vectors(ref_root):
     for basis in ("sto-3g", "6-31gs", "cc-pvdz"):
         z = np.load(os.path.join(data, "prop_h2o_%s.npz" % basis))
         np.savez_compressed(os.path.join(HERE, "ref_prop_h2o_%s.npz" % basis),
-                            **{k: z[k] for k in ("D", "D2", "J", "J2", "K", "K2")})
+                            **{k: z[k] for k in ("D", "D2", "J", "J2", "K", "K2", "Jgr", "Jgr2", "Jgr3", "Jgr4",
+                                                  "Kgr", "Kgr2", "Kgr3", "Kgr4")})
         z = np.load(os.path.join(data, "ewald_h2o_%s.npz" % basis))
         keep = [k for k in z.files if k.split("_")[0] in ("D", "D2", "J", "J2", "K", "K2")]
         np.savez_compressed(os.path.join(HERE, "ref_ewald_h2o_%s.npz" % basis), **{k: z[k] for k in keep})

@@ -42,3 +42,22 @@ def test_oracle_ewald(ls, golden_dir, basis):
         D, D2 = z["D_" + name], z["D2_" + name]
         assert np.max(abs(ref.coulomb(pl, pl, D, 1e-14, 1e-14, s, o) - z["J_" + name])) < 1e-12
         assert np.max(abs(ref.exchange(pl, pl, D2, False, 1e-14, 1e-14, s, o) - z["K2_" + name])) < 1e-12
+
+
+@pytest.mark.parametrize("basis", ["sto-3g", "6-31gs", "cc-pvdz"])
+def test_oracle_gradients(ls, golden_dir, basis):
+    """IntBox::coulombGrad / exchangeGrad of the reference build against the
+    reference's gradient vectors (prop_int.py:142-214, tolerance 1e-9): the
+    symmetric and the general (D12 != D34, D13/D24 symmetry flags) branches."""
+    _, rb = _ref_basis(ls, golden_dir, basis)
+    z = np.load(os.path.join(golden_dir, "ref_prop_h2o_%s.npz" % basis))
+    pl = ref.RefPairs(rb, rb, True, 1e-14)
+    D, D2 = z["D"], z["D2"]
+    assert np.max(abs(ref.coulomb_grad(pl, D) - z["Jgr"])) < 1e-9
+    assert np.max(abs(ref.coulomb_grad(pl, D2) - z["Jgr2"])) < 1e-9
+    assert np.max(abs(ref.coulomb_grad(pl, D, D2) - z["Jgr3"])) < 1e-9
+    assert np.max(abs(ref.coulomb_grad(pl, D2, D) - z["Jgr4"])) < 1e-9
+    assert np.max(abs(ref.exchange_grad(pl, D) - z["Kgr"])) < 1e-9
+    assert np.max(abs(ref.exchange_grad(pl, D2, None, False, False) - z["Kgr2"])) < 1e-9
+    assert np.max(abs(ref.exchange_grad(pl, D, D2, True, False) - z["Kgr3"])) < 1e-9
+    assert np.max(abs(ref.exchange_grad(pl, D2, D, False, True) - z["Kgr4"])) < 1e-9
