@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--carbons", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuned re-timing")
     ap.add_argument("--no-merge", action="store_true",
                     help="alkane: K over the primitives as given (the reference's exact quartet set) instead of "
                          "the merged twins")
@@ -358,6 +359,21 @@ def run_ours(args):
         ls.set_merge(True)
         exact = {"fp64_ms": ex64 / args.steps, "fp64_ms_k": exk64 / args.steps, "mixed_ms": exmx / args.steps,
                  "mixed_ms_k": exkmx / args.steps}
+    # the autotuner's value: one tuning build per mode (candidate launch shapes timed per
+    # class), then the same timed steps with the tuned table
+    tuned = None
+    if not args.no_tune:
+        ls.set_autotune(True)
+        for mode in (ls.PREC_FP64, ls.PREC_MIXED):
+            ls.set_precision(mode)
+            step(THREDP)
+        ls.set_autotune(False)
+        torch.cuda.synchronize()
+        tu64, tuk64 = timed(ls.PREC_FP64, THREDP, args.steps)
+        tumx, tukmx = timed(ls.PREC_MIXED, THREDP, args.steps)
+        tuned = {"fp64_ms": tu64 / args.steps, "fp64_ms_k": tuk64 / args.steps, "mixed_ms": tumx / args.steps,
+                 "mixed_ms_k": tukmx / args.steps, "default_fp64_ms": ms64 / args.steps,
+                 "default_mixed_ms": msmx / args.steps}
     # e2e through the public host API (each call copies D host->device; J and K come back)
     Dt = ls.Tensor.array(D)
     e2e_ms = 0.0
@@ -422,6 +438,8 @@ def run_ours(args):
         # quartets below thresp (dE_merged_vs_exact_Eh at fixed density); "exact" is the same
         # step over the reference's exact quartet set
         "merged_s_exponents": merge, "dE_merged_vs_exact_Eh": dE_merge if merge else 0.0, "exact": exact,
+        # the same steps after one autotuning build (the headline keeps the default schedule)
+        "autotuned": tuned,
         # quartets: the reference's quartet set of the step (its J and K screens over the
         # primitives as given); quartets_computed: what the merged build evaluates
         "quartets": q_ref, "quartets_ref_j": st_ref["j_quartets"], "quartets_ref_k": st_ref["k_quartets"],
@@ -556,9 +574,21 @@ def run_batched(args):
             ms_graph = timed(g.launch)
             ms_direct = timed(step)
             del g
+            ms_tuned = None
+            if not args.no_tune and opname == "coulomb" and prec == "mixed":
+                # the autotuner's value on the headline pair: tune once, time the direct
+                # step, then put the default table back for the other operators
+                table = ls.get_tune_table()
+                ls.set_autotune(True)
+                step()
+                ls.set_autotune(False)
+                torch.cuda.synchronize()
+                ms_tuned = timed(step)
+                ls.set_tune_table(table)
             q = st["j_quartets"] + st["k_quartets"]
             results["%s/%s" % (opname, prec)] = {
-                "ms_per_step": ms_graph, "ms_per_step_direct": ms_direct, "quartets": q,
+                "ms_per_step": ms_graph, "ms_per_step_direct": ms_direct,
+                "ms_per_step_direct_autotuned": ms_tuned, "quartets": q,
                 "density_quartets": 4 * q,   # every launch serves 4 densities (64 = 16 groups of 4)
                 "quartets_fp32": st["quartets_fp32"], "quartets_per_s": q / (ms_graph * 1e-3),
                 "density_quartets_per_s": 4 * q / (ms_graph * 1e-3),

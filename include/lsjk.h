@@ -237,6 +237,32 @@ int lsjk_coulomb_grad(lsjk_context* ctx, int nterm, const double* scales, const 
                       const lsjk_pairlist* pl, const double* D12, const double* D34, float thresp, float thredp,
                       double* G);
 
+/* One-electron integrals on the device, replacing IntBox::overlapCPU,
+ * kineticCPU and potentialCPU (src/lightspeed/intbox.hpp overlap/kinetic/
+ * potential; CPU kernels src/cpp/intbox/cpu/overlap.cpp, kinetic.cpp,
+ * potential.cpp): out (host, nao1 x nao2 of the pair list's bases, row-major)
+ * += S, T, or V = sum_C -Z_C <a| O(r - C) |b> for natom point charges xyzc
+ * (natom x 4: x, y, z, Z) under the Ewald operator. Every primitive pair of
+ * the list contributes (no further screening), as in the reference. */
+int lsjk_overlap(lsjk_context* ctx, const lsjk_pairlist* pl, double* out);
+int lsjk_kinetic(lsjk_context* ctx, const lsjk_pairlist* pl, double* out);
+int lsjk_potential(lsjk_context* ctx, int nterm, const double* scales, const double* omegas, const lsjk_pairlist* pl,
+                   int natom, const double* xyzc, double* out);
+
+/* K nuclear gradient, replaces IntBox::exchangeGrad (src/lightspeed/intbox.hpp:1095-1160,
+ * src/cpp/intbox/intbox.cpp:519-588; CPU kernels src/cpp/intbox/cpu/exchange_grad.cpp):
+ * G (natom x 3, row-major, host) += sum_{pqrs} D13_pr d(pq|rs)/dR D24_qs over a
+ * symmetric pair list; D13, D24 are host nao x nao matrices. D13symm, D24symm
+ * and Dsame are the reference's promises (symmetric D13, symmetric D24, D13 ==
+ * D24): they select which equal terms the reference skips and doubles, so the
+ * sum does not depend on them here and every quartet is computed. FP64
+ * throughout (thredp is ignored, as on the reference's CPU path); quartets
+ * screened like K (B_12 B_34 max|D24 block| >= thresp). LSJK_EINVAL for a
+ * non-symmetric list. */
+int lsjk_exchange_grad(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                       const lsjk_pairlist* pl, const double* D13, const double* D24, int D13symm, int D24symm,
+                       int Dsame, float thresp, float thredp, double* G);
+
 /* ---- CUDA graphs: capture the builds issued through the *_device entry
  * points between lsjk_graph_begin and lsjk_graph_end on the context stream,
  * then replay them with one lsjk_graph_launch (an SCF iteration's J+K as one

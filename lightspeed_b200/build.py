@@ -63,7 +63,7 @@ def gen_sources(force=False):
 def cuda_units():
     """(object name, source, extra flags) for every translation unit."""
     units = []
-    for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "mlp"):
+    for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "kgrad", "oneint", "mlp"):
         units.append((name, os.path.join(CSRC, name + ".cu"), []))
     # bra Hermite classes 0..2*LMAX, and 2*LMAX+1 for the gradients
     for lb in range(2 * LMAX + 2):

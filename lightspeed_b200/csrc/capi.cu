@@ -731,6 +731,98 @@ int lsjk_coulomb_grad(lsjk_context* ctx, int nterm, const double* scales, const 
     });
 }
 
+namespace {
+
+void one_electron_host(lsjk_context* ctx, int kind, const lsjk_pairlist* pl, const lsjk::Ewald* ew, int natom,
+                       const double* xyzc, double* out)
+{
+    if (!ctx || !pl || !out || (kind == 2 && natom > 0 && !xyzc)) throw lsjk::Error(LSJK_EINVAL, "null argument");
+    if (natom < 0) throw lsjk::Error(LSJK_EINVAL, "natom < 0");
+    lsjk::Context* c = &ctx->c;
+    set_device(*c);
+    const lsjk::PairList* p = &pl->p;
+    check_lmax(p);
+    const lsjk::Basis *b1 = p->b1, *b2 = p->b2;
+    const size_t nX = (size_t) b1->nao * b2->nao, nC = (size_t) b1->ncart * b2->ncart;
+    const size_t nq = kind == 2 ? (size_t) 4 * natom : 0;
+    c->scratch_reset();
+    double* dX = ctx->dev(nX + nq);
+    double* dq = dX + nX;
+    double* h = ctx->io_host.ensure(nX + nq);
+    if (nq) {
+        std::memcpy(h + nX, xyzc, sizeof(double) * nq);
+        LSJK_CUDA(cudaMemcpyAsync(dq, h + nX, sizeof(double) * nq, cudaMemcpyHostToDevice, c->stream));
+    }
+    double* Xc = lsjk::take<double>(c, nC);
+    LSJK_CUDA(cudaMemsetAsync(Xc, 0, sizeof(double) * nC, c->stream));
+    LSJK_CUDA(cudaMemsetAsync(dX, 0, sizeof(double) * nX, c->stream));
+    lsjk::one_electron(c, kind, p, ew, dq, natom, Xc);
+    lsjk::cart_to_pure_acc(c, b1, b2, Xc, dX);
+    LSJK_CUDA(cudaMemcpyAsync(h, dX, sizeof(double) * nX, cudaMemcpyDeviceToHost, c->stream));
+    check_kernels(c);
+    for (size_t i = 0; i < nX; ++i) out[i] += h[i];
+}
+
+} // namespace
+
+int lsjk_overlap(lsjk_context* ctx, const lsjk_pairlist* pl, double* out)
+{
+    return guard([&] { one_electron_host(ctx, 0, pl, nullptr, 0, nullptr, out); });
+}
+
+int lsjk_kinetic(lsjk_context* ctx, const lsjk_pairlist* pl, double* out)
+{
+    return guard([&] { one_electron_host(ctx, 1, pl, nullptr, 0, nullptr, out); });
+}
+
+int lsjk_potential(lsjk_context* ctx, int nterm, const double* scales, const double* omegas, const lsjk_pairlist* pl,
+                   int natom, const double* xyzc, double* out)
+{
+    return guard([&] {
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        one_electron_host(ctx, 2, pl, &ew, natom, xyzc, out);
+    });
+}
+
+int lsjk_exchange_grad(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
+                       const lsjk_pairlist* pl, const double* D13, const double* D24, int D13symm, int D24symm,
+                       int Dsame, float thresp, float thredp, double* G)
+{
+    (void) thredp;   // FP64 throughout, as the reference's CPU gradient
+    return guard([&] {
+        if (!ctx || !pl || !D13 || !D24 || !G) throw lsjk::Error(LSJK_EINVAL, "null argument");
+        lsjk::Context* c = &ctx->c;
+        set_device(*c);
+        lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
+        lsjk::PairList* p = const_cast<lsjk::PairList*>(&pl->p);
+        check_lmax(p);
+        if (!p->symm) throw lsjk::Error(LSJK_EINVAL, "IntBox::exchangeGrad: pairlist must be symmetric");
+        lsjk::build_kinv(c, p);   // the exact list's rows (merged twins are a K-build option only)
+        const lsjk::Basis* b = p->b1;
+        const size_t nD = (size_t) b->nao * b->nao, nG = (size_t) b->natom * 3;
+        // all three promises: the reference's fully symmetric routine, which reads D13 alone
+        // (intbox.cpp:553-564); otherwise its general routine over D13 and D24
+        const bool canon = D13symm && D24symm && Dsame;
+        const bool same = canon || D13 == D24;
+        c->scratch_reset();
+        double* dD = ctx->dev(2 * nD + nG);
+        double* dG = dD + 2 * nD;
+        double* h = ctx->io_host.ensure(2 * nD + nG);
+        std::memcpy(h, D13, sizeof(double) * nD);
+        if (!same) std::memcpy(h + nD, D24, sizeof(double) * nD);
+        LSJK_CUDA(cudaMemcpyAsync(dD, h, sizeof(double) * 2 * nD, cudaMemcpyHostToDevice, c->stream));
+        LSJK_CUDA(cudaMemsetAsync(dG, 0, sizeof(double) * nG, c->stream));
+        double* D13c = lsjk::take<double>(c, (size_t) b->ncart * b->ncart);
+        double* D24c = same ? D13c : lsjk::take<double>(c, (size_t) b->ncart * b->ncart);
+        lsjk::pure_to_cart(c, b, b, dD, D13c);
+        if (!same) lsjk::pure_to_cart(c, b, b, dD + nD, D24c);
+        lsjk::exchange_grad(c, ew, p, D13c, D24c, canon, dG, thresp);
+        LSJK_CUDA(cudaMemcpyAsync(h, dG, sizeof(double) * nG, cudaMemcpyDeviceToHost, c->stream));
+        check_kernels(c);
+        for (size_t i = 0; i < nG; ++i) G[i] += h[i];
+    });
+}
+
 int lsjk_graph_begin(lsjk_context* ctx)
 {
     return guard([&] {

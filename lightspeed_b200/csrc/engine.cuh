@@ -171,6 +171,9 @@ struct KInvData {
     DBuf<int> pt1, pseg;               // partner's second target (-1: none) and target group
     DBuf<double> pw0, pw1;             // partner's weights in its targets
     DBuf<float> pw0_32, pw1_32;
+    DBuf<double> pe;                   // partner's exponent (the K gradient's derivatives)
+    DBuf<int> patom;                   // partner's atom
+    DBuf<int> pidx;                    // partner's primitive index
 };
 
 struct PairList {
@@ -316,6 +319,12 @@ struct Ewald {
     std::vector<double> alpha, omega;   // terms with alpha != 0 and omega != 0
 };
 
+// One-electron integrals over a pair list (oneint.cu), added into the device
+// Cartesian matrix Xcart (ncart1 x ncart2): kind 0 overlap, 1 kinetic, 2 the
+// nuclear potential of natom charges xyzc (x, y, z, Z) under the operator ew.
+void one_electron(Context* ctx, int kind, const PairList* pl, const Ewald* ew, const double* xyzc, int natom,
+                  double* Xcart);
+
 // densities per batched J or K build (one quartet loop for all of them)
 constexpr int kJBatchMax = 4;
 
@@ -338,5 +347,11 @@ void coulomb_grad(Context* ctx, const Ewald& ew, const PairList* pl, const doubl
 void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                     const double* const* Dcart, const double* const* Dscr, double* const* Kcart, int ng,
                     bool d24symm, bool flip_ok, float thresp, float thredp, const Basis* kb1, const Basis* kb3);
+// K nuclear gradient (FP64): G[atom][xyz] += sum D13 d(12|34)/dR D24 over the
+// K-invert quartets of a symmetric pair list (K-invert rows built), Cartesian
+// densities in, device G (natom x 3) accumulated. canon: the quartet screen of
+// the reference's fully symmetric routine (D13 == D24 symmetric).
+void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D13cart, const double* D24cart,
+                   bool canon, double* G, float thresp);
 
 } // namespace lsjk

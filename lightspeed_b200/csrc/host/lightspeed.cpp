@@ -326,6 +326,25 @@ std::shared_ptr<Tensor> IntBox::coulombGrad(const std::shared_ptr<ResourceList>&
     return out;
 }
 
+std::shared_ptr<Tensor> IntBox::exchangeGrad(const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ewald,
+                                             const std::shared_ptr<PairList>& pl, const std::shared_ptr<Tensor>& D13,
+                                             const std::shared_ptr<Tensor>& D24, bool D13symm, bool D24symm,
+                                             bool Dsame, float thresp, float thredp,
+                                             const std::shared_ptr<Tensor>& G)
+{
+    const size_t n = pl->basis1()->nao();
+    D13->shape_error({n, n});
+    D24->shape_error({n, n});
+    auto out = out_tensor(G, pl->basis1()->natom(), 3, "G");
+    const double* d13 = D13->data().data();
+    const double* d24 = D13 == D24 ? d13 : D24->data().data();
+    check_rc(lsjk_exchange_grad(Engine::instance().ctx(), (int) ewald->scales().size(), ewald->scales().data(),
+                                ewald->omegas().data(), pl->device_handle(), d13, d24, D13symm, D24symm, Dsame,
+                                thresp, thredp, out->data().data()),
+             "IntBox::exchangeGrad");
+    return out;
+}
+
 std::shared_ptr<Tensor> IntBox::exchange(const std::shared_ptr<ResourceList>& resources,
                                          const std::shared_ptr<Ewald>& ewald,
                                          const std::shared_ptr<PairList>& pl12, const std::shared_ptr<PairList>& pl34,

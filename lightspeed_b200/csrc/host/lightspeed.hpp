@@ -215,6 +215,16 @@ public:
                                                const std::shared_ptr<Tensor>& D12,
                                                const std::shared_ptr<Tensor>& D34, float thresp, float thredp,
                                                const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>());
+    // K nuclear gradient (src/lightspeed/intbox.hpp:1095-1160): G (natom, 3) +=
+    // sum D13 d(12|34) D24 over a symmetric pair list. D13symm, D24symm, Dsame
+    // are accepted as the reference's promises; the sum does not depend on them.
+    static std::shared_ptr<Tensor> exchangeGrad(const std::shared_ptr<ResourceList>& resources,
+                                                const std::shared_ptr<Ewald>& ewald,
+                                                const std::shared_ptr<PairList>& pairlist,
+                                                const std::shared_ptr<Tensor>& D13,
+                                                const std::shared_ptr<Tensor>& D24, bool D13symm, bool D24symm,
+                                                bool Dsame, float thresp, float thredp,
+                                                const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>());
     static std::shared_ptr<Tensor> exchange(const std::shared_ptr<ResourceList>& resources,
                                             const std::shared_ptr<Ewald>& ewald,
                                             const std::shared_ptr<PairList>& pairlist12,

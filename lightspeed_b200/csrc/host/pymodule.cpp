@@ -167,6 +167,10 @@ PYBIND11_MODULE(_lightspeed, m)
         .def_static("coulombGrad", &IntBox::coulombGrad, py::arg("resources"), py::arg("ewald"), py::arg("pairlist"),
                     py::arg("D12"), py::arg("D34"), py::arg("thresp"), py::arg("thredp"),
                     py::arg("G") = std::shared_ptr<Tensor>(), py::call_guard<py::gil_scoped_release>())
+        .def_static("exchangeGrad", &IntBox::exchangeGrad, py::arg("resources"), py::arg("ewald"),
+                    py::arg("pairlist"), py::arg("D13"), py::arg("D24"), py::arg("D13symm"), py::arg("D24symm"),
+                    py::arg("Dsame"), py::arg("thresp"), py::arg("thredp"), py::arg("G") = std::shared_ptr<Tensor>(),
+                    py::call_guard<py::gil_scoped_release>())
         .def_static("exchange", &IntBox::exchange, py::arg("resources"), py::arg("ewald"), py::arg("pairlist12"),
                     py::arg("pairlist34"), py::arg("D24"), py::arg("D24symm"), py::arg("thresp"),
                     py::arg("thredp"), py::arg("K13") = std::shared_ptr<Tensor>(),
@@ -183,7 +187,7 @@ PYBIND11_MODULE(_lightspeed, m)
                     py::arg("pairlist34"), py::arg("C1"), py::arg("C2"), py::arg("C3"), py::arg("C4"),
                     py::arg("thresp"), py::arg("thredp"), py::arg("I") = std::shared_ptr<Tensor>(),
                     py::call_guard<py::gil_scoped_release>())
-        // one-electron integrals for the SCF drivers (host C++)
+        // one-electron integrals for the SCF drivers (device kernels, oneint.cu)
         .def_static("overlap", [](const std::shared_ptr<ResourceList>&, const std::shared_ptr<PairList>& pl,
                                   const std::shared_ptr<Tensor>& S) { return OneInt::overlap(pl, S); },
                     py::arg("resources"), py::arg("pairlist"), py::arg("S") = std::shared_ptr<Tensor>(),

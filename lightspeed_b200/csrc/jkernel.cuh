@@ -156,17 +156,19 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         if (B0 * Bj < A.thresp) break;
         const float est = Bi * Bj;
         const bool pass = act && est >= A.thresp;
-        const bool dp = pass && est >= thr_dp;
-        const bool sp = pass && !dp;
+        // one precision per warp and ket: FP64 while any lane's estimate reaches thredp
+        // (those lanes need it; the others get FP64 too rather than a second, FP32
+        // pass of the warp over the same ket), FP32 after. The kets are in bound
+        // order, so the warp switches once.
+        const bool dp = __any_sync(0xffffffffu, pass && est >= thr_dp);
         const double* r = A.krec + (long) j * S;
-        if (__any_sync(0xffffffffu, dp)) {
-            if (dp) {
+        if (dp) {
+            if (pass) {
                 ++nq;
                 j_quartet64<LB, LK, NG>(A, tab, p, Px, Py, Pz, r, jp);
             }
-        }
-        if (__any_sync(0xffffffffu, sp)) {
-            if (sp) {
+        } else if (__any_sync(0xffffffffu, pass)) {
+            if (pass) {
                 ++nq32;
                 j_quartet32<LB, LK, NG>(A, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
             }

@@ -83,4 +83,43 @@ struct KArgs {
 template <int L1, int L2, int L3, int L4>
 void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32);
 
+// Arguments of the K gradient kernel (kgrad.cu): the K build's task list and
+// bound-ordered partner rows of one exact pair list, with each partner's
+// exponent and atom, one D13 and one D24 (Cartesian), and G (natom x 3).
+struct KGradArgs {
+    const KTask* tasks;
+    const int* ntask;
+    unsigned* queue;
+    const int *r12s, *r12l, *r34s, *r34l;
+    const float *b12, *b34;
+    const double *kab12, *p12, *ip12, *px12, *py12, *pz12, *ax12, *ay12, *az12, *pe12;
+    const int *cart12, *atom12, *pidx12;
+    const double *kab34, *p34, *ip34, *px34, *py34, *pz34, *ax34, *ay34, *az34, *pe34;
+    const int *cart34, *atom34, *pidx34;
+    BasisView b2, b4;
+    const double* D13;
+    int ld13;
+    const double* D24;
+    int ld24;
+    double* G;
+    const KScalars* sc;
+    float thr_lo;               // thresp: quartets with bound12 bound34 max|D24 block| >= thresp
+    // canon != 0: the reference's fully symmetric gradient, whose screen reads the
+    // D block of (max(prim1, prim2), max(prim3, prim4)) for every quartet: dblk holds
+    // max|D block| per primitive pair (nprim x nprim), and the tasks carry the global max
+    const double* dblk;
+    int nprim;
+    int canon;
+    const double* rys;          // FP64 Rys table block of the rule one quantum up
+    const double* asym_t;
+    const double* asym_w;
+    int nbin;
+    double tmax;
+    int nterm;
+    double alpha[4], omega[4];
+};
+
+// One (L1 L2|L3 L4) class of the K gradient (cap: the class's task capacity).
+void launch_k_grad(Context* ctx, const KGradArgs& A, long cap, int L1, int L2, int L3, int L4);
+
 } // namespace lsjk

@@ -64,6 +64,19 @@ __global__ void k_absmax(const double* __restrict__ X, long n, unsigned long lon
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long) __double_as_longlong(m));
 }
 
+// out[i * nprim + j] = max |D| over the Cartesian block of primitives (i, j).
+__global__ void k_prim_blockmax(const double* __restrict__ D, int ld, BasisView b, double* __restrict__ out)
+{
+    const long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
+    if (k >= (long) b.nprim * b.nprim) return;
+    const int i = (int) (k / b.nprim), j = (int) (k % b.nprim);
+    const int ci = b.cart[i], cj = b.cart[j], ni = ncart_of(b.L[i]), nj = ncart_of(b.L[j]);
+    double m = 0.0;
+    for (int a = 0; a < ni; ++a)
+        for (int c = 0; c < nj; ++c) m = fmax(m, fabs(D[(long) (ci + a) * ld + cj + c]));
+    out[k] = m;
+}
+
 // thre12 = thresp / (max_bound(pl34) * D24max), thre34 likewise (exchange.cpp:54-71)
 __global__ void k_kscalars(KScalars* S, float thresp, double maxb12, double maxb34)
 {
@@ -96,6 +109,7 @@ struct TaskGenArgs {
     int* ntask_hi;
     float thredp;
     int split;
+    int global_dmax;               // tasks carry the global max|D| (sc) instead of their block's
 };
 
 // Append one task per lane that wants one to the list of its class c: the
@@ -127,7 +141,9 @@ __global__ void k_task_gen(TaskGenArgs A)
     const int L4 = valid ? A.b4.L[i4] : 0;
     // largest |D24| over the pair's block and the batch's densities
     double dmax = 0.0;
-    if (valid) {
+    if (A.global_dmax) {
+        dmax = __longlong_as_double((long long) A.sc->dmax_bits);
+    } else if (valid) {
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
         const int n2 = ncart_of(L2), n4 = ncart_of(L4);
         for (int g = 0; g < A.ng; ++g)
@@ -437,6 +453,132 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
             ctx->stats.kernel_launches++;
         }
     }
+}
+
+// The K gradient over the K build's quartet set (exchange_grad.cpp:523-760:
+// bound12 >= thre12, bound34 >= thre34, bound12 bound34 max|D24 block| >=
+// thresp), every (prim2, prim4) pair and every partner pair -- the D13/D24
+// symmetry flags of the reference's general routine only choose which equal
+// terms it skips and doubles, so the sum is the same without them. `canon`:
+// the reference's fully symmetric routine (D13symm, D24symm and Dsame;
+// exchange_grad.cpp:17-470), which computes one representative per set of
+// equal terms and screens all of them with the representative's D block;
+// the same sum over the same quartets here.
+void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D13cart, const double* D24cart,
+                   bool canon, double* G, float thresp)
+{
+    if (ew.alpha.size() > 4) throw Error(LSJK_EINVAL, "exchange_grad: at most 4 Ewald terms");
+    cudaStream_t s = ctx->stream;
+    const Basis* b = pl->b1;
+    if (!b->nprim || !pl->kdat.nent) return;
+    KScalars* sc = take<KScalars>(ctx, 1);
+    LSJK_CUDA(cudaMemsetAsync(sc, 0, sizeof(KScalars), s));
+    const long nd = (long) b->ncart * b->ncart;
+    k_absmax<<<std::min<long>(nblk(nd, 256), 1184), 256, 0, s>>>(D24cart, nd, &sc->dmax_bits);
+    k_kscalars<<<1, 1, 0, s>>>(sc, thresp, pl->max_bound, pl->max_bound);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches += 2;
+
+    int cnt[kNL] = {0};
+    for (int L : b->L) cnt[L]++;
+    std::vector<long> off(kNCombo + 1, 0);
+    for (int L1 = 0; L1 < kNL; ++L1)
+        for (int L2 = 0; L2 < kNL; ++L2)
+            for (int L3 = 0; L3 < kNL; ++L3)
+                for (int L4 = 0; L4 < kNL; ++L4) off[combo_index(L1, L2, L3, L4) + 1] = (long) cnt[L2] * cnt[L4];
+    for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
+    KTask* tasks = take<KTask>(ctx, off[kNCombo]);
+    int* ntask = take<int>(ctx, kNCombo);
+    unsigned* queue = take<unsigned>(ctx, kNCombo);
+    LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * kNCombo, s));
+    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * kNCombo, s));
+
+    TaskGenArgs T{};
+    T.b2 = b->view();
+    T.b4 = b->view();
+    for (int a = 0; a < kNL; ++a)
+        for (int c = 0; c < kNL; ++c) {
+            T.r12.start[a][c] = T.r34.start[a][c] = pl->kinv[a][c].row_start.p;
+            T.r12.len[a][c] = T.r34.len[a][c] = pl->kinv[a][c].row_len.p;
+        }
+    T.pb12 = T.pb34 = pl->kdat_b.pbound.p;
+    T.Dc[0] = D24cart;
+    T.ng = 1;
+    T.ld4 = b->ncart;
+    T.d24symm = 0;
+    T.thresp = thresp;
+    T.sc = sc;
+    T.tasks = tasks;
+    for (int c = 0; c < kNCombo; ++c) T.cap_off[c] = off[c];
+    T.ntask = ntask;
+    T.global_dmax = canon ? 1 : 0;
+    double* dblk = nullptr;
+    if (canon) {
+        const long np2 = (long) b->nprim * b->nprim;
+        dblk = take<double>(ctx, np2);
+        k_prim_blockmax<<<nblk(np2, 256), 256, 0, s>>>(D24cart, b->ncart, b->view(), dblk);
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+    }
+    dim3 grid(b->nprim, nblk(b->nprim, 128));
+    k_task_gen<<<grid, 128, 0, s>>>(T);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
+
+    const KInvData& d = pl->kdat_b;   // partners 1 and 3 both in bound order
+    for (int L1 = 0; L1 < kNL; ++L1)
+        for (int L2 = 0; L2 < kNL; ++L2)
+            for (int L3 = 0; L3 < kNL; ++L3)
+                for (int L4 = 0; L4 < kNL; ++L4) {
+                    const int c = combo_index(L1, L2, L3, L4);
+                    const long cap = off[c + 1] - off[c];
+                    if (!cap || !pl->kinv[L2][L1].row_len.p || !pl->kinv[L4][L3].row_len.p) continue;
+                    const int NR = (L1 + L2 + L3 + L4 + 1) / 2 + 1;   // one quantum up
+                    KGradArgs A{};
+                    A.tasks = tasks + off[c];
+                    A.ntask = ntask + c;
+                    A.queue = queue + c;
+                    A.r12s = pl->kinv[L2][L1].row_start.p;
+                    A.r12l = pl->kinv[L2][L1].row_len.p;
+                    A.r34s = pl->kinv[L4][L3].row_start.p;
+                    A.r34l = pl->kinv[L4][L3].row_len.p;
+                    A.b12 = A.b34 = d.pbound.p;
+                    A.kab12 = A.kab34 = d.kab.p;
+                    A.p12 = A.p34 = d.p.p;
+                    A.ip12 = A.ip34 = d.ip.p;
+                    A.px12 = A.px34 = d.px.p;
+                    A.py12 = A.py34 = d.py.p;
+                    A.pz12 = A.pz34 = d.pz.p;
+                    A.ax12 = A.ax34 = d.ax.p;
+                    A.ay12 = A.ay34 = d.ay.p;
+                    A.az12 = A.az34 = d.az.p;
+                    A.pe12 = A.pe34 = d.pe.p;
+                    A.cart12 = A.cart34 = d.pcart.p;
+                    A.atom12 = A.atom34 = d.patom.p;
+                    A.pidx12 = A.pidx34 = d.pidx.p;
+                    A.dblk = dblk;
+                    A.nprim = b->nprim;
+                    A.canon = canon ? 1 : 0;
+                    A.b2 = A.b4 = b->view();
+                    A.D13 = D13cart;
+                    A.ld13 = b->ncart;
+                    A.D24 = D24cart;
+                    A.ld24 = b->ncart;
+                    A.G = G;
+                    A.sc = sc;
+                    A.thr_lo = thresp;
+                    A.rys = ctx->rys64.p + kRysOffset[NR];
+                    A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
+                    A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
+                    A.nbin = kRysNbin[NR];
+                    A.tmax = kRysTmax[NR];
+                    A.nterm = (int) ew.alpha.size();
+                    for (int t = 0; t < A.nterm; ++t) {
+                        A.alpha[t] = ew.alpha[t];
+                        A.omega[t] = ew.omega[t];
+                    }
+                    launch_k_grad(ctx, A, cap, L1, L2, L3, L4);
+                }
 }
 
 } // namespace lsjk

@@ -220,8 +220,9 @@ __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ 
                             float* __restrict__ ax32, float* __restrict__ ay32, float* __restrict__ az32,
                             int* __restrict__ pcart, float* __restrict__ pb, int* __restrict__ pt1,
                             int* __restrict__ pseg, double* __restrict__ pw0, double* __restrict__ pw1,
-                            float* __restrict__ pw0_32, float* __restrict__ pw1_32,
-                            int* __restrict__ rstart, int* __restrict__ rlen, int nrow)
+                            float* __restrict__ pw0_32, float* __restrict__ pw1_32, double* __restrict__ pe,
+                            int* __restrict__ patom, int* __restrict__ pidx, int* __restrict__ rstart,
+                            int* __restrict__ rlen, int nrow)
 {
     long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -245,6 +246,9 @@ __global__ void k_kinv_fill(const KEnt* __restrict__ e, const int* __restrict__ 
     pw1[k] = bpart.w1[j];
     pw0_32[k] = (float) bpart.w0[j];
     pw1_32[k] = (float) bpart.w1[j];
+    pe[k] = ej;
+    patom[k] = bpart.atom[j];
+    pidx[k] = j;
     pb[k] = t.b;
     long r = (long) t.cls * nrow + i;
     bool first = (k == 0);
@@ -398,6 +402,7 @@ void build_kinv(Context* ctx, PairList* pl)
     kd.pz32.alloc(m); kd.ax32.alloc(m); kd.ay32.alloc(m); kd.az32.alloc(m);
     kd.pcart.alloc(m); kd.pbound.alloc(m);
     kd.pt1.alloc(m); kd.pseg.alloc(m); kd.pw0.alloc(m); kd.pw1.alloc(m); kd.pw0_32.alloc(m); kd.pw1_32.alloc(m);
+    kd.pe.alloc(m); kd.patom.alloc(m); kd.pidx.alloc(m);
     unsigned long long* ka = take<unsigned long long>(ctx, m);
     unsigned long long* kas = take<unsigned long long>(ctx, m);
     int* va = take<int>(ctx, m);
@@ -428,8 +433,8 @@ void build_kinv(Context* ctx, PairList* pl)
                                             kd.ip.p, kd.px.p, kd.py.p, kd.pz.p, kd.ax.p, kd.ay.p, kd.az.p,
                                             kd.kab32.p, kd.p32.p, kd.ip32.p, kd.px32.p, kd.py32.p, kd.pz32.p,
                                             kd.ax32.p, kd.ay32.p, kd.az32.p, kd.pcart.p, kd.pbound.p, kd.pt1.p,
-                                            kd.pseg.p, kd.pw0.p, kd.pw1.p, kd.pw0_32.p, kd.pw1_32.p, rstart,
-                                            rlen, nrow);
+                                            kd.pseg.p, kd.pw0.p, kd.pw1.p, kd.pw0_32.p, kd.pw1_32.p, kd.pe.p,
+                                            kd.patom.p, kd.pidx.p, rstart, rlen, nrow);
     LSJK_CUDA(cudaGetLastError());
     // the bound-ordered copy (same rows, so the same row tables)
     KInvData& kb_ = pl->kdat_b;
@@ -440,7 +445,7 @@ void build_kinv(Context* ctx, PairList* pl)
     kb_.pz32.alloc(m); kb_.ax32.alloc(m); kb_.ay32.alloc(m); kb_.az32.alloc(m);
     kb_.pcart.alloc(m); kb_.pbound.alloc(m);
     kb_.pt1.alloc(m); kb_.pseg.alloc(m); kb_.pw0.alloc(m); kb_.pw1.alloc(m); kb_.pw0_32.alloc(m);
-    kb_.pw1_32.alloc(m);
+    kb_.pw1_32.alloc(m); kb_.pe.alloc(m); kb_.patom.alloc(m); kb_.pidx.alloc(m);
     int* rstart_b = take<int>(ctx, (long) kNL * kNL * nrow);
     int* rlen_b = take<int>(ctx, (long) kNL * kNL * nrow);
     LSJK_CUDA(cudaMemsetAsync(rstart_b, 0, sizeof(int) * kNL * kNL * nrow, s));
@@ -450,7 +455,7 @@ void build_kinv(Context* ctx, PairList* pl)
                                             kb_.az.p, kb_.kab32.p, kb_.p32.p, kb_.ip32.p, kb_.px32.p, kb_.py32.p,
                                             kb_.pz32.p, kb_.ax32.p, kb_.ay32.p, kb_.az32.p, kb_.pcart.p,
                                             kb_.pbound.p, kb_.pt1.p, kb_.pseg.p, kb_.pw0.p, kb_.pw1.p, kb_.pw0_32.p,
-                                            kb_.pw1_32.p, rstart_b, rlen_b, nrow);
+                                            kb_.pw1_32.p, kb_.pe.p, kb_.patom.p, kb_.pidx.p, rstart_b, rlen_b, nrow);
     LSJK_CUDA(cudaGetLastError());
     for (int a = 0; a < kNL; ++a)
         for (int b = 0; b < kNL; ++b) {

@@ -36,6 +36,12 @@ def lib():
         _lib.ref_kinetic.argtypes = [vp, vp, ip]
         _lib.ref_potential.argtypes = [vp, ip, vp, vp, ip, vp, vp, ip]
         _lib.ref_rys.argtypes = [ip, ip, vp, vp, vp]
+        # every handle and pointer argument typed: an untyped Python int goes through
+        # ctypes as a 32-bit C int, which cuts a 64-bit handle short
+        _lib.ref_basis_nao.argtypes = [vp]
+        _lib.ref_basis_ncart.argtypes = [vp]
+        _lib.ref_coulomb_grad.argtypes = [vp, ip, vp, vp, vp, vp, ip, fp, fp, vp, ip]
+        _lib.ref_exchange_grad.argtypes = [vp, ip, vp, vp, vp, vp, ip, ip, ip, fp, fp, vp, ip]
     return _lib
 
 
@@ -60,8 +66,8 @@ class RefBasis:
                                      _p(a["atom"]))
         if not self.h:
             _check(1)
-        self.nao = lib().ref_basis_nao(ctypes.c_void_p(self.h))
-        self.ncart = lib().ref_basis_ncart(ctypes.c_void_p(self.h))
+        self.nao = lib().ref_basis_nao(self.h)
+        self.ncart = lib().ref_basis_ncart(self.h)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -33,6 +33,9 @@ def shim():
     ref.lib()   # the reference objects' library first (the shim links it)
     lib = ctypes.CDLL(SHIM)
     lib.shim_last_error.restype = ctypes.c_char_p
+    vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    # typed arguments: an untyped Python int would go through as a 32-bit C int
+    lib.shim_jk.argtypes = [ip, vp, vp, ip, vp, vp, vp, ip, fp, fp, ip, vp]
     return lib
 
 
