@@ -161,7 +161,8 @@ int lsjk_pairlist_export(const lsjk_pairlist* pl, int* L1, int* L2, int* prim1,
  * O(r) = sum_i scales[i] erf(omegas[i] r)/r (omega = -1: 1/r), ndens densities
  * at once. IntBox::coulomb (src/lightspeed/intbox.hpp:761-771,
  * src/cpp/intbox/intbox.cpp:213-250). D34[k] is (nao3, nao4), J12[k] is
- * (nao1, nao2), host memory. */
+ * (nao1, nao2), host memory. Up to 64 densities go through one build: one
+ * kernel launch per class for all of them (more are taken 64 at a time). */
 int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
                  const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
                  const double* const* D34, float thresp, float thredp, double* const* J12);
@@ -169,7 +170,10 @@ int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const doubl
 /* ---- K: K13 += sum_qs (pq|rs) D24_qs with the reference's density-screened
  * K-invert ordering. IntBox::exchange (src/lightspeed/intbox.hpp:817-828,
  * src/cpp/intbox/intbox.cpp:290-330). D24symm requires basis 2 == basis 4
- * (LSJK_EINVAL otherwise, like src/cpp/intbox/cpu/exchange.cpp:74-76). */
+ * (LSJK_EINVAL otherwise, like src/cpp/intbox/cpu/exchange.cpp:74-76).
+ * Up to 64 densities go through one build: groups of four share a task list
+ * screened with their largest |D24|, and one kernel launch per class and
+ * precision pass serves every group (more are taken 64 at a time). */
 int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const double* omegas,
                   const lsjk_pairlist* pl12, const lsjk_pairlist* pl34, int ndens,
                   const double* const* D24, int D24symm, float thresp, float thredp,
@@ -216,7 +220,7 @@ int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const double* scal
  * (src/cpp/intbox/mo_eri.cpp:10-157): one J build per (i, j), with i >= j
  * when sym12, of the density C1[:,i] C2[:,j]^T over pl34's pairs (bra pl34,
  * ket pl12, mo_eri.cpp:74-118), then I[i][j] = C3^T J C4. Here the densities
- * are formed on the device and go through the batched J path 16 at a time;
+ * are formed on the device and go through the batched J path 64 at a time;
  * J never leaves the device. The flags stand for the reference's
  * pointer-identity tests and select its symmetrisations (mo_eri.cpp:121-155):
  * sym12 for C1 == C2, sym34 for C3 == C4, sym1234 for C1 == C3 and C2 == C4.

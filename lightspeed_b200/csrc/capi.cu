@@ -136,16 +136,16 @@ void screening_densities(lsjk::Context* ctx, const lsjk::Basis* o3, const lsjk::
     }
 }
 
-// One J build for ng (1..4) densities that share the quartet loop, device
-// pointers in and out.
+// One J build for ng (1..kMaxDens) densities (one launch per class for all of
+// them), device pointers in and out.
 void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12,
                    const lsjk::PairList* pl34, const double* const* Dpure, double* const* Jpure, int ng,
                    float thresp, float thredp)
 {
     ctx->scratch_reset();
     const lsjk::Basis *b1 = pl12->b1, *b2 = pl12->b2, *b3 = pl34->b1, *b4 = pl34->b2;
-    double* Dc[lsjk::kJBatchMax];
-    double* Jc[lsjk::kJBatchMax];
+    double* Dc[lsjk::kMaxDens];
+    double* Jc[lsjk::kMaxDens];
     for (int g = 0; g < ng; ++g) {
         Dc[g] = lsjk::take<double>(ctx, (size_t) b3->ncart * b4->ncart);
         Jc[g] = lsjk::take<double>(ctx, (size_t) b1->ncart * b2->ncart);
@@ -157,8 +157,9 @@ void coulomb_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairLi
     for (int g = 0; g < ng; ++g) lsjk::cart_to_pure_acc(ctx, b1, b2, Jc[g], Jpure[g]);
 }
 
-// One K build for ng (1..4) densities sharing the quartet integrals, device
-// pointers in and out. Over twins D24 lives in the twins' slots of bases 2
+// One K build for ng (1..kMaxDens) densities (groups of four share task lists
+// and quartet integrals; one launch per class and pass), device pointers in
+// and out. Over twins D24 lives in the twins' slots of bases 2
 // and 4, while K13 is accumulated straight into the Cartesian spaces of the
 // caller's bases 1 and 3 (each partner primitive carries its output targets).
 void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairList* pl12_in,
@@ -169,15 +170,15 @@ void exchange_group(lsjk::Context* ctx, const lsjk::Ewald& ew, const lsjk::PairL
     const lsjk::PairList* pl34 = effective(ctx, pl34_in);
     ctx->scratch_reset();
     const lsjk::Basis *b1 = pl12_in->b1, *b2 = pl12->b2, *b3 = pl34_in->b1, *b4 = pl34->b2;
-    double* Dc[lsjk::kJBatchMax];
-    double* Kc[lsjk::kJBatchMax];
+    double* Dc[lsjk::kMaxDens];
+    double* Kc[lsjk::kMaxDens];
     for (int g = 0; g < ng; ++g) {
         Dc[g] = lsjk::take<double>(ctx, (size_t) b2->ncart * b4->ncart);
         Kc[g] = lsjk::take<double>(ctx, (size_t) b1->ncart * b3->ncart);
         lsjk::pure_to_cart(ctx, b2, b4, Dpure[g], Dc[g]);
         LSJK_CUDA(cudaMemsetAsync(Kc[g], 0, sizeof(double) * b1->ncart * b3->ncart, ctx->stream));
     }
-    double* Ds[lsjk::kJBatchMax];
+    double* Ds[lsjk::kMaxDens];
     screening_densities(ctx, pl12_in->b2, pl34_in->b2, b2, b4, Dpure, ng, Ds);
     if (!ew.alpha.empty() && pl12->npair && pl34->npair)
         lsjk::exchange_build(ctx, ew, pl12, pl34, Dc, Ds[0] ? Ds : nullptr, Kc, ng, d24symm, flip_ok, thresp,
@@ -592,9 +593,9 @@ int lsjk_coulomb_device(lsjk_context* ctx, int nterm, const double* scales, cons
         lsjk::Ewald ew = make_ewald(nterm, scales, omegas);
         check_lmax(&pl12->p);
         check_lmax(&pl34->p);
-        for (int k0 = 0; k0 < ndens; k0 += lsjk::kJBatchMax)
+        for (int k0 = 0; k0 < ndens; k0 += lsjk::kMaxDens)
             coulomb_group(&ctx->c, ew, &pl12->p, &pl34->p, D34 + k0, J12 + k0,
-                          std::min(lsjk::kJBatchMax, ndens - k0), thresp, thredp);
+                          std::min(lsjk::kMaxDens, ndens - k0), thresp, thredp);
     });
 }
 
@@ -611,9 +612,9 @@ int lsjk_exchange_device(lsjk_context* ctx, int nterm, const double* scales, con
         bool d24 = false, flip = false;
         exchange_prepare(&ctx->c, const_cast<lsjk::PairList*>(&pl12->p), const_cast<lsjk::PairList*>(&pl34->p),
                          D24symm, &d24, &flip);
-        for (int k0 = 0; k0 < ndens; k0 += lsjk::kJBatchMax)
+        for (int k0 = 0; k0 < ndens; k0 += lsjk::kMaxDens)
             exchange_group(&ctx->c, ew, &pl12->p, &pl34->p, D24 + k0, d24, flip, K13 + k0,
-                           std::min(lsjk::kJBatchMax, ndens - k0), thresp, thredp);
+                           std::min(lsjk::kMaxDens, ndens - k0), thresp, thredp);
     });
 }
 
@@ -631,15 +632,15 @@ int lsjk_coulomb(lsjk_context* ctx, int nterm, const double* scales, const doubl
         check_lmax(&pl34->p);
         const size_t nD = (size_t) pl34->p.b1->nao * pl34->p.b2->nao;
         const size_t nJ = (size_t) pl12->p.b1->nao * pl12->p.b2->nao;
-        const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
+        const int G = std::max(1, std::min(lsjk::kMaxDens, ndens));
         double* dD = ctx->dev((nD + nJ) * G);
         double* dJ = dD + nD * G;
         double* hD = ctx->io_host.ensure((nD + nJ) * G);
         double* hJ = hD + nD * G;
         for (int k0 = 0; k0 < ndens; k0 += G) {
             const int ng = std::min(G, ndens - k0);
-            const double* dp[lsjk::kJBatchMax];
-            double* jp[lsjk::kJBatchMax];
+            const double* dp[lsjk::kMaxDens];
+            double* jp[lsjk::kMaxDens];
             for (int g = 0; g < ng; ++g) {
                 dp[g] = dD + g * nD;
                 jp[g] = dJ + g * nJ;
@@ -671,15 +672,15 @@ int lsjk_exchange(lsjk_context* ctx, int nterm, const double* scales, const doub
                          &d24, &flip);
         const size_t nD = (size_t) pl12->p.b2->nao * pl34->p.b2->nao;
         const size_t nK = (size_t) pl12->p.b1->nao * pl34->p.b1->nao;
-        const int G = std::max(1, std::min(lsjk::kJBatchMax, ndens));
+        const int G = std::max(1, std::min(lsjk::kMaxDens, ndens));
         double* dD = ctx->dev((nD + nK) * G);
         double* dK = dD + nD * G;
         double* hD = ctx->io_host.ensure((nD + nK) * G);
         double* hK = hD + nD * G;
         for (int k0 = 0; k0 < ndens; k0 += G) {
             const int ng = std::min(G, ndens - k0);
-            const double* dp[lsjk::kJBatchMax];
-            double* kp[lsjk::kJBatchMax];
+            const double* dp[lsjk::kMaxDens];
+            double* kp[lsjk::kMaxDens];
             for (int g = 0; g < ng; ++g) {
                 dp[g] = dD + g * nD;
                 kp[g] = dK + g * nK;
@@ -1012,7 +1013,7 @@ extern "C" int lsjk_coulomb_device_noalloc(lsjk_context* ctx, int nterm, const d
 
 namespace {
 
-constexpr int kEriBatch = 16;   // (i, j) densities per round of J builds
+constexpr int kEriBatch = lsjk::kMaxDens;   // (i, j) densities per J build
 
 struct EriPairs {
     int i[kEriBatch], j[kEriBatch];
@@ -1122,15 +1123,15 @@ extern "C" int lsjk_eri_j(lsjk_context* ctx, int nterm, const double* scales, co
             }
             if (n34) LSJK_CUDA(cudaMemsetAsync(dJ.p, 0, sizeof(double) * n34 * ng, s));
             // J over pl34's pairs of each density on pl12's bases (bra pl34, ket pl12: mo_eri.cpp:88-95)
-            for (int g0 = 0; g0 < ng; g0 += lsjk::kJBatchMax) {
-                const int m = std::min(lsjk::kJBatchMax, ng - g0);
-                const double* dp[lsjk::kJBatchMax];
-                double* jp[lsjk::kJBatchMax];
-                for (int g = 0; g < m; ++g) {
-                    dp[g] = dD.p + (g0 + g) * n12;
-                    jp[g] = dJ.p + (g0 + g) * n34;
+            {
+                static_assert(kEriBatch <= lsjk::kMaxDens, "one J build per batch of densities");
+                const double* dp[kEriBatch];
+                double* jp[kEriBatch];
+                for (int g = 0; g < ng; ++g) {
+                    dp[g] = dD.p + g * n12;
+                    jp[g] = dJ.p + g * n34;
                 }
-                coulomb_group(c, ew, &pl34->p, &pl12->p, dp, jp, m, thresp, thredp);
+                coulomb_group(c, ew, &pl34->p, &pl12->p, dp, jp, ng, thresp, thredp);
             }
             // L = C3^T J C4 (mo_eri.cpp:96-110)
             if (nao4 > 0 && nao3 > 0) {

@@ -325,8 +325,12 @@ struct Ewald {
 void one_electron(Context* ctx, int kind, const PairList* pl, const Ewald* ew, const double* xyzc, int natom,
                   double* Xcart);
 
-// densities per batched J or K build (one quartet loop for all of them)
+// densities whose quartets one J thread or K lane evaluates together (one
+// quadrature, several contractions)
 constexpr int kJBatchMax = 4;
+// densities per J or K build: one launch per class and pass serves all of them
+// (K: groups of kJBatchMax densities share a task list; J: grid.z over groups)
+constexpr int kMaxDens = 64;
 
 // J for ng (1..4) densities at once; batched densities share the quartets
 // (screened with the largest |D| of the batch).

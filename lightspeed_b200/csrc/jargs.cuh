@@ -26,9 +26,8 @@ struct JArgs {
     int mixed;                // 1: quartets with estimate < thredp run in FP32
     float thredp;
     int chunk;                // ket pairs per CTA (grid.y = ceil(nket / chunk))
-    int ng;                   // densities of the build (1..kJBatch)
-    int slots;                // density blocks per ket record (1, or kJBatch for a batched build)
-    int g0;                   // first density of this launch (a launch covers g0 .. g0 + NG - 1)
+    int ng;                   // densities of the build (1..kMaxDens); CTA z covers NG of them
+    int slots;                // density blocks per ket record (= ng)
     long jbra_stride;         // distance between the densities' bra accumulators
     int nterm;
     double alpha[4], omega[4];

@@ -33,11 +33,11 @@ inline unsigned nblk(long n, int t) { return (unsigned) ((n + t - 1) / t); }
 
 // ---- 1. ket screening -------------------------------------------------------
 
-// The densities of one launch (1..kJBatch), passed by value.
+// The densities of one build (1..kMaxDens), passed by value.
 struct DSet {
-    const double* d[kJBatch];
+    const double* d[kMaxDens];
     int n;       // densities present
-    int slots;   // record slots (1, or kJBatch for a batched launch)
+    int slots;   // record slots (= n)
 };
 
 __global__ void k_ket_screen(const int* __restrict__ p1, const int* __restrict__ p2,
@@ -586,11 +586,11 @@ KetSet prepare_kets(Context* ctx, const PairList* pl12, const PairList* pl34, co
 void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const PairList* pl34,
                    const double* const* Dcart, double* const* Jcart, int ng, float thresp, float thredp)
 {
-    if (ng < 1 || ng > kJBatch) throw Error(LSJK_EINVAL, "coulomb_build: 1..4 densities per launch");
+    if (ng < 1 || ng > kMaxDens) throw Error(LSJK_EINVAL, "coulomb_build: 1..64 densities per build");
     DSet DS{};
     for (int g = 0; g < ng; ++g) DS.d[g] = Dcart[g];
     DS.n = ng;
-    DS.slots = ng == 1 ? 1 : kJBatch;
+    DS.slots = ng;
     cudaStream_t s = ctx->stream;
     const Basis *b1 = pl12->b1, *b2 = pl12->b2;
     unsigned long long* qcnt = ctx->counters.p;                          // FP64 J classes
@@ -650,7 +650,6 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             }
             A.ng = ng;
             A.slots = DS.slots;
-            A.g0 = 0;
             A.jbra_stride = (long) jb.n * nherm_of(LB);
             A.nterm = (int) ew.alpha.size();
             for (int t = 0; t < A.nterm; ++t) {
@@ -761,7 +760,6 @@ static void coulomb_grad_bra(Context* ctx, const Ewald& ew, const PairList* pl, 
             A.chunk = chunk;
             A.ng = 1;
             A.slots = 1;
-            A.g0 = 0;
             A.jbra_stride = (long) jb.n * H1;
             A.nterm = (int) ew.alpha.size();
             for (int t = 0; t < A.nterm; ++t) {

@@ -14,7 +14,7 @@ namespace lsjk {
 // One J quartet (bra pair in registers, ket record r) accumulated into jp,
 // for the NG densities of the record (the Hermite integrals R_tuv are shared).
 template <int LB, int LK, int NG>
-__device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, double p, double Px, double Py,
+__device__ __forceinline__ void j_quartet64(const JArgs& A, int g0, const double* tab, double p, double Px, double Py,
                                             double Pz, const double* __restrict__ r, double (*jp)[nherm_of(LB)])
 {
     constexpr int L = LB + LK, HK = nherm_of(LK);
@@ -44,14 +44,14 @@ __device__ __forceinline__ void j_quartet64(const JArgs& A, const double* tab, d
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g)
-            if (A.g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r + 4 + (A.g0 + g) * HK, jp[g]);
+            if (g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r + 4 + (g0 + g) * HK, jp[g]);
     }
 }
 
-// Densities of one J launch for a bra class: the batched kernel keeps NG x HB
-// FP64 accumulators per thread (and as many FP32 ones), so the heavy bra
-// classes take fewer densities per launch (more launches over the same ket
-// records) instead of spilling.
+// Densities per CTA for a bra class: the batched kernel keeps NG x HB FP64
+// accumulators per thread (and as many FP32 ones), so the heavy bra classes
+// take fewer densities per CTA (more CTA z-slices over the same ket records)
+// instead of spilling.
 template <int LB>
 __host__ __device__ constexpr int j_batch() { return nherm_of(LB) <= 4 ? kJBatch : (nherm_of(LB) <= 10 ? 2 : 1); }
 
@@ -64,7 +64,7 @@ constexpr float kBoysSwitch32 = (float) (LSJK_BOYS_TMAX - LSJK_BOYS_TMAX / LSJK_
 // else in FP32 except the Boys function at T >= kBoysSwitch32, which is
 // evaluated in FP64 by its asymptotic form), added to the FP64 accumulators.
 template <int LB, int LK, int NG>
-__device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, float p,
+__device__ __forceinline__ void j_quartet32(const JArgs& A, int g0, const float* tab, float p,
                                             double Px, double Py, double Pz, const double* __restrict__ r,
                                             const float* __restrict__ r32, double (*jp)[nherm_of(LB)])
 {
@@ -106,7 +106,7 @@ __device__ __forceinline__ void j_quartet32(const JArgs& A, const float* tab, fl
         }
 #pragma unroll
         for (int g = 0; g < NG; ++g)
-            if (A.g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4 + (A.g0 + g) * HK, jq[g]);
+            if (g0 + g < A.ng) jq_dispatch<LB, LK>(a, X, Y, Z, r32 + 4 + (g0 + g) * HK, jq[g]);
     }
 #pragma unroll
     for (int g = 0; g < NG; ++g)
@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
     __shared__ __align__(128) float tab32[LSJK_BOYS_NBIN * 8];
     __shared__ __align__(8) uint64_t mbar[2];
     const int nb = *A.nbra, nk = *A.nket;
+    const int g0 = blockIdx.z * NG;   // the densities g0 .. g0 + NG - 1 of the build
     const int i0 = blockIdx.x * kJThreads;
     const int j0 = blockIdx.y * A.chunk;
     if (i0 >= nb || j0 >= nk) return;
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 #pragma unroll
         for (int t = 0; t < HB; ++t) jp[g][t] = 0.0;
     long nq = 0, nq32 = 0;
+    const int nd = min(NG, A.ng - g0);   // statistics count density-quartets
     const int j1 = min(j0 + A.chunk, nk);
     for (int j = j0; j < j1; ++j) {
         const float Bj = A.kbound[j];
@@ -164,13 +166,13 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         const double* r = A.krec + (long) j * S;
         if (dp) {
             if (pass) {
-                ++nq;
-                j_quartet64<LB, LK, NG>(A, tab, p, Px, Py, Pz, r, jp);
+                nq += nd;
+                j_quartet64<LB, LK, NG>(A, g0, tab, p, Px, Py, Pz, r, jp);
             }
         } else if (__any_sync(0xffffffffu, pass)) {
             if (pass) {
-                ++nq32;
-                j_quartet32<LB, LK, NG>(A, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
+                nq32 += nd;
+                j_quartet32<LB, LK, NG>(A, g0, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
             }
         }
     }
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
 #pragma unroll
             for (int t = 0; t < HB; ++t) {
                 const double v = jp[g][t];
-                if (v != 0.0 && A.g0 + g < A.ng) atomicAdd(&A.jbra[(A.g0 + g) * A.jbra_stride + (long) i * HB + t], v);
+                if (v != 0.0 && g0 + g < A.ng) atomicAdd(&A.jbra[(g0 + g) * A.jbra_stride + (long) i * HB + t], v);
             }
     }
     // quartet counts for the statistics
@@ -198,22 +200,18 @@ template <int LB, int LK>
 void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full)
 {
     if (nbra_full == 0 || nket_full == 0) return;
-    dim3 grid((nbra_full + kJThreads - 1) / kJThreads, (nket_full + A.chunk - 1) / A.chunk);
+    // one launch for all densities: CTA z takes NG of them over the same ket
+    // records (NG = the class's batch when there are that many, else 1)
     constexpr int NGB = j_batch<LB>();
-    // densities g0 .. g0 + NG - 1 per launch, over the same ket records
-    for (int g0 = 0; g0 < A.ng;) {
-        JArgs B = A;
-        B.g0 = g0;
-        if (A.ng - g0 >= NGB && NGB > 1) {
-            k_coulomb<LB, LK, NGB><<<grid, kJThreads, 0, ctx->stream>>>(B);
-            g0 += NGB;
-        } else {
-            k_coulomb<LB, LK, 1><<<grid, kJThreads, 0, ctx->stream>>>(B);
-            g0 += 1;
-        }
-        LSJK_CUDA(cudaGetLastError());
-        ctx->stats.kernel_launches++;
-    }
+    const bool batched = NGB > 1 && A.ng >= NGB;
+    const int NG = batched ? NGB : 1;
+    dim3 grid((nbra_full + kJThreads - 1) / kJThreads, (nket_full + A.chunk - 1) / A.chunk, (A.ng + NG - 1) / NG);
+    if (batched)
+        k_coulomb<LB, LK, NGB><<<grid, kJThreads, 0, ctx->stream>>>(A);
+    else
+        k_coulomb<LB, LK, 1><<<grid, kJThreads, 0, ctx->stream>>>(A);
+    LSJK_CUDA(cudaGetLastError());
+    ctx->stats.kernel_launches++;
 }
 
 

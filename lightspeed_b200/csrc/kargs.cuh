@@ -7,12 +7,14 @@ namespace lsjk {
 
 constexpr int kKThreads = 128;
 constexpr int kKWarps = kKThreads / 32;
-constexpr int kKBatch = 4;        // densities per K build (one task list, screened with their largest |D|)
+constexpr int kKBatch = 4;        // densities of a group (one task list, screened with their largest |D|)
 
-// One (prim2, prim4) task: the K-invert rows of prim2 (partners 1) and prim4
-// (partners 3) and the largest |D24| over the pair's Cartesian block.
+// One (prim2, prim4) task of a density group: the K-invert rows of prim2
+// (partners 1) and prim4 (partners 3) and the largest |D24| over the pair's
+// Cartesian block and the group's densities (primitive indices < 65536).
 struct KTask {
-    int i2, i4;
+    int i2;
+    unsigned short i4, grp;
     double dmax;
 };
 
@@ -52,11 +54,14 @@ struct KArgs {
     const double* w1_34;
     const float* b34;
     BasisView b2, b4;         // indexed primitives (centres, cartIdx)
-    const double* Dc[kKBatch];   // D24 of each density of the launch (Cartesian, ld4)
+    const double* Dc[kMaxDens];  // D24 of each density of the build (Cartesian, ld4)
     int ld4;
-    double* Kc[kKBatch];         // K13 of each density (Cartesian output space of bases 1 and 3, ld3)
+    double* Kc[kMaxDens];        // K13 of each density (Cartesian output space of bases 1 and 3, ld3)
     int ld3;
-    int ng;                      // densities: launch_k splits them over kernel launches
+    int ng;                      // densities of the build, in groups of kKBatch (the tasks' grp)
+    int nsub;                    // densities of a group / NG of the launch, rounded up: the launch
+                                 // runs its tasks nsub times (task index t + sub * ntask), sub-slot
+                                 // `sub` taking densities grp * kKBatch + sub * NG + [0, NG)
     int flip;
     int gc;                      // partners may carry two output targets (merged twins): the kernel
                                  // variant with two target blocks for s-type partners

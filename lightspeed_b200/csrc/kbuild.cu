@@ -95,13 +95,13 @@ struct TaskGenArgs {
     KRowTables r12, r34;
     const float* pb12;
     const float* pb34;
-    const double* Dc[kKBatch];
+    const double* Dc[kMaxDens];    // screening densities of the build; CTA z = group of kKBatch
     int ng;
     int ld4;
     int d24symm;
     float thresp;
     const KScalars* sc;
-    KTask* tasks;                  // per-combo regions
+    KTask* tasks;                  // per-combo regions (all groups' tasks of a class in one region)
     long cap_off[kNCombo];         // region offsets (by value: graph-capturable)
     int* ntask;                    // per-combo counts
     // mixed precision: tasks whose first quartet reaches thredp, the only ones the FP64 pass can use
@@ -132,6 +132,8 @@ __global__ void k_task_gen(TaskGenArgs A)
 {
     const int i2 = blockIdx.x;
     const int i4 = blockIdx.y * blockDim.x + threadIdx.x;
+    const int grp = blockIdx.z;   // densities grp * kKBatch .. + kKBatch - 1
+    const int g0 = grp * kKBatch, g1 = min(A.ng, g0 + kKBatch);
     // exchange.cpp:137-139 (prim2 <= prim4 for a symmetric D24); lanes out of
     // range stay for the warp-wide votes below
     const bool valid = i4 < A.b4.nprim && !(A.d24symm && i2 > i4);
@@ -146,7 +148,7 @@ __global__ void k_task_gen(TaskGenArgs A)
     } else if (valid) {
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
         const int n2 = ncart_of(L2), n4 = ncart_of(L4);
-        for (int g = 0; g < A.ng; ++g)
+        for (int g = g0; g < g1; ++g)
             for (int a = 0; a < n2; ++a)
                 for (int b = 0; b < n4; ++b) dmax = fmax(dmax, fabs(A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b]));
     }
@@ -169,7 +171,7 @@ __global__ void k_task_gen(TaskGenArgs A)
                 }
             }
             const int c = combo_index(L1, L2, L3, L4);
-            const KTask t{i2, i4, dmax};
+            const KTask t{i2, (unsigned short) i4, (unsigned short) grp, dmax};
             const unsigned wm = __ballot_sync(0xffffffffu, want);
             if (want) append_task(wm, c, A.cap_off[c], A.ntask, A.tasks, t);
             const bool hi = want && A.split && (double) (b12 * b34) * dmax >= (double) A.thredp;
@@ -236,7 +238,8 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
 {
     // screens read Dscr (max|D24| estimates); the integrals contract with Dcart
     const double* const* Dscr = Dscr_in ? Dscr_in : Dcart;
-    if (ng < 1 || ng > kKBatch) throw Error(LSJK_EINVAL, "exchange_build: 1..4 densities per build");
+    if (ng < 1 || ng > kMaxDens) throw Error(LSJK_EINVAL, "exchange_build: 1..64 densities per build");
+    const int ngroup = (ng + kKBatch - 1) / kKBatch;
     cudaStream_t s = ctx->stream;
     const int b1c = kb1->ncart;   // K13 lives in the output spaces of bases 1 and 3
     const Basis *b2 = pl12->b2, *b3 = kb3, *b4 = pl34->b2;
@@ -262,18 +265,18 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
             for (int L3 = 0; L3 < kNL; ++L3)
                 for (int L4 = 0; L4 < kNL; ++L4) {
                     int c = combo_index(L1, L2, L3, L4);
-                    off[c + 1] = (long) cnt2[L2] * cnt4[L4];
+                    off[c + 1] = (long) cnt2[L2] * cnt4[L4] * ngroup;
                 }
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
     int* ntask = take<int>(ctx, 2 * kNCombo);   // all tasks, then the FP64-pass tasks
     KTask* tasks_hi = mixed ? take<KTask>(ctx, off[kNCombo]) : nullptr;
-    unsigned* queue = take<unsigned>(ctx, 2 * kNCombo * kKBatch);   // per class, pass and launch
+    unsigned* queue = take<unsigned>(ctx, 2 * kNCombo);   // per class and pass (one launch each)
     unsigned long long* qcnt = ctx->counters.p + kNJClass;                          // FP64 K classes
     unsigned long long* qcnt32 = ctx->counters.p + kNJClass + kNKClass + kNJClass;  // FP32 K classes
     LSJK_CUDA(cudaMemsetAsync(ntask, 0, sizeof(int) * 2 * kNCombo, s));
-    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo * kKBatch, s));
+    LSJK_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned) * 2 * kNCombo, s));
 
     TaskGenArgs G{};
     G.b2 = b2->view();
@@ -303,7 +306,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     if (b2->nprim && b4->nprim && pl12->kdat.nent && pl34->kdat.nent) {
         // prim2 varies fastest over the blocks, so the lists interleave prim2 rows: warps taking
         // neighbouring tasks then mostly add into different K13 rows
-        dim3 grid(b2->nprim, nblk(b4->nprim, 128));
+        dim3 grid(b2->nprim, nblk(b4->nprim, 128), ngroup);
         k_task_gen<<<grid, 128, 0, s>>>(G);
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches++;
@@ -375,7 +378,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     }
                     const float inf = __builtin_huge_valf();
                     // FP64 pass: estimate >= thredp (mixed) or >= thresp (FP64 mode)
-                    A.queue = queue + (long) c * kKBatch;
+                    A.queue = queue + c;
                     if (mixed) {
                         // FP64 pass: only the tasks that can reach thredp
                         A.tasks = tasks_hi + off[c];
@@ -403,7 +406,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                             slot = cnd;
                             float ms = 1e30f;
                             for (int rep = 0; rep < 2; ++rep) {
-                                LSJK_CUDA(cudaMemsetAsync(T.queue, 0, sizeof(unsigned) * kKBatch, s));
+                                LSJK_CUDA(cudaMemsetAsync(T.queue, 0, sizeof(unsigned), s));
                                 LSJK_CUDA(cudaEventRecord(ctx->ev0, s));
                                 launch_k1(ctx, T, cap, L1, L2, L3, L4, fp32);
                                 LSJK_CUDA(cudaEventRecord(ctx->ev1, s));
@@ -418,7 +421,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                             }
                         }
                         slot = bestc;
-                        LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned) * kKBatch, s));
+                        LSJK_CUDA(cudaMemsetAsync(X.queue, 0, sizeof(unsigned), s));
                     };
                     if (ctx->tuning) tune(A, false);
                     {
@@ -430,7 +433,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         // FP32 pass: thresp <= estimate < thredp, over all tasks
                         A.tasks = tasks + off[c];
                         A.ntask = ntask + c;
-                        A.queue = queue + (long) (kNCombo + c) * kKBatch;
+                        A.queue = queue + kNCombo + c;
                         A.thr_lo = thresp;
                         A.thr_hi = thredp;
                         A.rys = ctx->rys32.p + kRysOffset[NR];

@@ -13,8 +13,10 @@
 // and issues one FP64 atomic per element when the segment ends (for a
 // symmetric D24 only the untransposed one: the build symmetrises K13 after
 // the class kernels).
-// Up to k_batch densities share a launch: the integrals of a quartet are
-// formed once and contracted with each density's D24 block.
+// Up to k_batch densities share a lane: the integrals of a quartet are
+// formed once and contracted with each density's D24 block; one launch per
+// class and pass serves every density of the build (groups of kKBatch with
+// their own task lists, each run once per sub-slot of k_batch densities).
 // Screens (per quartet, exactly the reference's set):
 //   bound12 >= thre12, bound34 >= thre34,
 //   thr_lo <= double(float(bound12*bound34)) * max|D24 block| < thr_hi
@@ -70,6 +72,7 @@ struct alignas(16) KHdr {
     float tlo, thi;         // float thresholds on bound12 * bound34 for this task's max|D24|
     float b12max;           // largest bound of the partner-1 row
     float wsym;             // 1/2 for a diagonal task of a symmetric D24, else 1
+    int dbase, dn;          // densities dbase .. dbase + dn - 1 of the build (the task's sub-slot)
 };
 
 // Lane l copies entry kb + l of the row (if it exists) into dst[l].
@@ -112,7 +115,7 @@ __device__ __forceinline__ void stage_ent(KEnt<R>* dst, const KRows<R>& d, const
     cp_async4(&o->seg, seg + e);
 }
 
-// Densities per launch for a class: up to kKBatch while a per-density
+// Densities per lane for a class: up to kKBatch while a per-density
 // register weight, N1*N3*(2+w) + N2*N4*w with w the 32-bit registers of one R
 // (the segment accumulators and D24 block, with headroom for the
 // accumulation's temporaries; chosen by measurement), stays within 64; 1 above.
@@ -224,7 +227,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     __shared__ __align__(8) uint64_t mbar;
     __shared__ KEnt<R> ring_all[kKWarps][2][32];
     __shared__ KHdr hdr_all[kKWarps][kKGrab];
-    const int ntask = *A.ntask;
+    const int ntask1 = *A.ntask;
+    const int ntask = ntask1 * A.nsub;   // the task list once per density sub-slot
     // the grid is sized for the class's task capacity; CTAs whose warps cannot
     // get a task leave before staging the quadrature table
     if ((long) blockIdx.x * kKWarps >= ntask) return;
@@ -256,9 +260,13 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
         const int nt = min(grab, ntask - t0);
         __syncwarp();   // the previous grab's headers have been read
         if (lane < nt) {
-            const KTask T = A.tasks[t0 + lane];
+            const int tv = t0 + lane;
+            const int sub = tv / ntask1;
+            const KTask T = A.tasks[tv - sub * ntask1];
             const int i2 = T.i2, i4 = T.i4;
             KHdr h;
+            h.dbase = T.grp * kKBatch + sub * NG;
+            h.dn = max(0, min(NG, min(A.ng, (T.grp + 1) * kKBatch) - h.dbase));
             h.dRx = A.b2.x[i2] - A.b4.x[i4];
             h.dRy = A.b2.y[i2] - A.b4.y[i4];
             h.dRz = A.b2.z[i2] - A.b4.z[i4];
@@ -282,7 +290,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                     const float b = A.b34[h.s34 + mid];
                     if (b >= thre34 && h.b12max * b >= h.tlo) lo = mid + 1; else hi = mid;
                 }
-                h.n34 = lo;
+                h.n34 = h.dn > 0 ? lo : 0;   // a sub-slot past the group's densities: no work
             }
             // symmetric D24 (A.flip): the transposed contribution of a task with i2 != i4 is
             // not written here; the build adds K13 to its transpose afterwards, and tasks with
@@ -301,10 +309,12 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
             while (pos < nt && hdr[pos].n34 == 0) ++pos;
             if (pos >= nt) break;
             const int s12 = hdr[pos].s12, n12 = hdr[pos].n12, c2 = hdr[pos].c2;
+            // the pack's densities (its tasks share prim2 and the density sub-slot)
+            const int dbase = hdr[pos].dbase, dn = hdr[pos].dn;
             int my_task = -1, my_k = 0;
             {
                 int filled = 0, at = pos, k0 = koff;
-                while (filled < 32 && at < nt && hdr[at].s12 == s12) {
+                while (filled < 32 && at < nt && hdr[at].s12 == s12 && hdr[at].dbase == dbase) {
                     const int n = hdr[at].n34;
                     const int len = min(n - k0, 32 - filled);
                     if (lane >= filled && lane < filled + len) {
@@ -343,7 +353,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                 for (int a = 0; a < N2; ++a)
 #pragma unroll
                     for (int b = 0; b < N4; ++b)
-                        Dblk[g][a * N4 + b] = in3 ? (R) A.Dc[g][(long) (c2 + a) * A.ld4 + c4 + b] : R(0);
+                        Dblk[g][a * N4 + b] = in3 && (NG == 1 || g < dn)
+                                                  ? (R) A.Dc[dbase + g][(long) (c2 + a) * A.ld4 + c4 + b] : R(0);
             {
                 // partner 3 of this lane (all loads of the entry issue together)
                 float b34 = 0.0f;
@@ -387,7 +398,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                     if (any) {
 #pragma unroll
                         for (int g = 0; g < NG; ++g) {
-                            double* Kc = A.Kc[g];
+                            if (NG > 1 && g >= dn) break;   // (a pack of one density always has it)
+                            double* Kc = A.Kc[dbase + g];
 #pragma unroll
                             for (int a = 0; a < N1; ++a)
 #pragma unroll
@@ -464,7 +476,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
                         if (!__any_sync(0xffffffffu, pass)) continue;
                         if (!pass) continue;
                         const KEnt<R> e = cur[j];
-                        ++nq;
+                        nq += dn;   // statistics count density-quartets
                         any = true;
                         if constexpr (G1 == 2) {
                             // one integral, added to both targets with the entry's weights
@@ -539,46 +551,38 @@ void launch_k_gc(Context* ctx, const KArgs& A, unsigned grid)
     launch_k_one<L1, L2, L3, L4, R, NG, false>(ctx, A, grid);
 }
 
-// One class, one precision pass, A.ng densities: launches of k_batch densities
-// while they last, then single-density launches. Each launch takes its own
-// work-queue counter (A.queue[launch index], zeroed by the caller).
+// One class, one precision pass, all A.ng densities in one launch: NG =
+// k_batch densities per lane when a group holds that many, else 1, and the
+// task list run once per sub-slot of NG densities of the groups.
 template <int L1, int L2, int L3, int L4>
 void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
 {
     if (cap == 0 || A.ng < 1) return;
-    long want = (cap + kKWarps - 1) / kKWarps;
+    const int per_group = std::min(A.ng, kKBatch);
     int per_sm = ctx->tune.k_ctas_per_sm[fp32 ? 1 : 0][L1][L2][L3][L4];
-    unsigned grid = (unsigned) std::min<long>(want, (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
+    auto grid_for = [&](int nsub) {
+        const long want = (cap * nsub + kKWarps - 1) / kKWarps;
+        return (unsigned) std::min<long>(want, (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
+    };
     KArgs B = A;
-    int g0 = 0, launch = 0;
-    while (g0 < A.ng) {
-        for (int g = 0; g < kKBatch; ++g) {
-            B.Dc[g] = g0 + g < A.ng ? A.Dc[g0 + g] : nullptr;
-            B.Kc[g] = g0 + g < A.ng ? A.Kc[g0 + g] : nullptr;
-        }
-        B.queue = A.queue + launch;
-        int used;
-        if (fp32) {
-            constexpr int NGf = k_batch<L1, L2, L3, L4, float>();
-            if (NGf > 1 && A.ng - g0 >= NGf) {
-                launch_k_gc<L1, L2, L3, L4, float, NGf>(ctx, B, grid);
-                used = NGf;
-            } else {
-                launch_k_gc<L1, L2, L3, L4, float, 1>(ctx, B, grid);
-                used = 1;
-            }
+    if (fp32) {
+        constexpr int NGf = k_batch<L1, L2, L3, L4, float>();
+        if (NGf > 1 && per_group >= NGf) {
+            B.nsub = (per_group + NGf - 1) / NGf;
+            launch_k_gc<L1, L2, L3, L4, float, NGf>(ctx, B, grid_for(B.nsub));
         } else {
-            constexpr int NGd = k_batch<L1, L2, L3, L4, double>();
-            if (NGd > 1 && A.ng - g0 >= NGd) {
-                launch_k_gc<L1, L2, L3, L4, double, NGd>(ctx, B, grid);
-                used = NGd;
-            } else {
-                launch_k_gc<L1, L2, L3, L4, double, 1>(ctx, B, grid);
-                used = 1;
-            }
+            B.nsub = per_group;
+            launch_k_gc<L1, L2, L3, L4, float, 1>(ctx, B, grid_for(B.nsub));
         }
-        g0 += used;
-        ++launch;
+    } else {
+        constexpr int NGd = k_batch<L1, L2, L3, L4, double>();
+        if (NGd > 1 && per_group >= NGd) {
+            B.nsub = (per_group + NGd - 1) / NGd;
+            launch_k_gc<L1, L2, L3, L4, double, NGd>(ctx, B, grid_for(B.nsub));
+        } else {
+            B.nsub = per_group;
+            launch_k_gc<L1, L2, L3, L4, double, 1>(ctx, B, grid_for(B.nsub));
+        }
     }
 }
 

@@ -1,8 +1,10 @@
 """Batched densities: IntBox.coulombMulti / exchangeMulti with several
 densities in one call against one call per density.
 
-A batched J launch shares its quartet loop between up to four densities and
-screens with the largest |D| of the batch, so it evaluates a superset of each
+A batched build serves all its densities with one launch per class (J: CTA
+z-slices of up to four densities; K: task lists per group of four densities,
+run once per sub-slot), shares each quartet between up to four densities and
+screens with the largest |D| of the group, so it evaluates a superset of each
 density's quartets: results agree with the per-density builds to the size of
 the quartets the single-density screen drops. At thresp = 1e-14 that is far
 below the 1e-10 elementwise FP64 tolerance. In mixed precision the batch also
@@ -77,6 +79,31 @@ def test_multi_fp64_vs_oracle(ls):
         for D, J in zip(Dn, Jm):
             Jr = ref.coulomb(rp, rp, D, 1e-14, 1e-14)
             assert np.max(abs(J.np - Jr)) < 1e-10
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
+
+
+def test_thirteen_densities_one_build_vs_oracle(ls):
+    """Thirteen densities in one build (four density groups, the last one
+    partial: every class kernel runs once over all groups and sub-slots)
+    against the oracle one density at a time, J and K, FP64."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("reference CPU IntBox not built")
+    ls.set_precision(ls.PREC_FP64)
+    try:
+        bas, pl = _system(ls)
+        res = ls.ResourceList.build()
+        ew = ls.Ewald([1.0], [-1.0])
+        Dn = _densities(13, bas.nao, 23)
+        Ds = [ls.Tensor.array(D) for D in Dn]
+        Jm = ls.IntBox.coulombMulti(res, ew, pl, pl, Ds, 1e-14, 1e-14)
+        Km = ls.IntBox.exchangeMulti(res, ew, pl, pl, Ds, False, 1e-14, 1e-14)
+        rb = ref.RefBasis(ref.prim_arrays(bas))
+        rp = ref.RefPairs(rb, rb, True, 1e-14)
+        for D, J, K in zip(Dn, Jm, Km):
+            assert np.max(abs(J.np - ref.coulomb(rp, rp, D, 1e-14, 1e-14))) < 1e-10
+            assert np.max(abs(K.np - ref.exchange(rp, rp, D, False, 1e-14, 1e-14))) < 1e-10
     finally:
         ls.set_precision(ls.PREC_MIXED)
 
