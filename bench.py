@@ -521,6 +521,21 @@ def run_batched(args):
     kptr = [Kd[k].data_ptr() for k in range(ndens)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     torch.cuda.synchronize()
+    if args.profile_step:
+        # one mixed-precision step of the bare operator between profiler start and stop
+        ew = ls.Ewald([1.0], [-1.0])
+        ls.set_precision(ls.PREC_MIXED)
+        for _ in range(max(args.warmup, 1)):
+            ls.coulomb_device(ew, pl, pl, dptr, jptr, thre, THREDP)
+            ls.exchange_device(ew, pl, pl, dptr, False, kptr, thre, THREDP)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        ls.coulomb_device(ew, pl, pl, dptr, jptr, thre, THREDP)
+        ls.exchange_device(ew, pl, pl, dptr, False, kptr, thre, THREDP)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_step": True, "workload": "batched, 64 densities, mixed, bare operator"}))
+        return 0
     results = {}
     ref = {}
     clocks = Clocks(local)

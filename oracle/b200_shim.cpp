@@ -1,6 +1,7 @@
 // The reference-side binding of the B200 engine: what a Lightspeed maintainer
 // adds to the reference so that IntBox::coulomb / IntBox::exchange
-// (src/lightspeed/intbox.hpp:761-771, :817-828) run on liblsjk.so, written
+// (src/lightspeed/intbox.hpp:761-771, :817-828) and their nuclear gradients
+// coulombGrad / exchangeGrad (:998-1008, :1147-1160) run on liblsjk.so, written
 // against the reference's own headers and types (Tensor, Basis, PairList,
 // Ewald, ResourceList) and compiled from them by oracle/Makefile (target
 // shim) into oracle/_ref/libls_b200shim.so. In the reference it would replace
@@ -139,6 +140,46 @@ std::shared_ptr<Tensor> exchange(const std::shared_ptr<ResourceList>&, const std
     return K;
 }
 
+// IntBox::coulombGrad's signature (src/lightspeed/intbox.hpp:998-1008): G
+// (natom x 3) accumulates; D12 and D34 the same object is the reference's
+// symmetric branch (one pointer passed on).
+std::shared_ptr<Tensor> coulombGrad(const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ewald,
+                                    const std::shared_ptr<PairList>& pl, const std::shared_ptr<Tensor>& D12,
+                                    const std::shared_ptr<Tensor>& D34, float thresp, float thredp,
+                                    const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>())
+{
+    const size_t n = pl->basis1()->nao(), natom = pl->basis1()->natom();
+    D12->shape_error({n, n});
+    D34->shape_error({n, n});
+    std::shared_ptr<Tensor> out = G ? G : std::make_shared<Tensor>(std::vector<size_t>{natom, 3});
+    out->shape_error({natom, 3});
+    const double* a = D12->data().data();
+    const double* b = D12 == D34 ? a : D34->data().data();
+    check(lsjk_coulomb_grad(ctx(), (int) ewald->scales().size(), ewald->scales().data(), ewald->omegas().data(),
+                            dev(pl), a, b, thresp, thredp, out->data().data()));
+    return out;
+}
+
+// IntBox::exchangeGrad's signature (src/lightspeed/intbox.hpp:1147-1160): the
+// three flags pass through (all three select the reference's fully symmetric
+// routine, which reads D13 alone).
+std::shared_ptr<Tensor> exchangeGrad(const std::shared_ptr<ResourceList>&, const std::shared_ptr<Ewald>& ewald,
+                                     const std::shared_ptr<PairList>& pl, const std::shared_ptr<Tensor>& D13,
+                                     const std::shared_ptr<Tensor>& D24, bool D13symm, bool D24symm, bool Dsame,
+                                     float thresp, float thredp,
+                                     const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>())
+{
+    const size_t n = pl->basis1()->nao(), natom = pl->basis1()->natom();
+    D13->shape_error({n, n});
+    D24->shape_error({n, n});
+    std::shared_ptr<Tensor> out = G ? G : std::make_shared<Tensor>(std::vector<size_t>{natom, 3});
+    out->shape_error({natom, 3});
+    check(lsjk_exchange_grad(ctx(), (int) ewald->scales().size(), ewald->scales().data(), ewald->omegas().data(),
+                             dev(pl), D13->data().data(), D24->data().data(), D13symm ? 1 : 0, D24symm ? 1 : 0,
+                             Dsame ? 1 : 0, thresp, thredp, out->data().data()));
+    return out;
+}
+
 } // namespace b200
 } // namespace lightspeed
 
@@ -179,6 +220,40 @@ int shim_jk(int which, void* pl12, void* pl34, int nterm, const double* scales, 
                                           : b200::coulomb(res, ew, p12, p34, Dt, thresp, thredp, O);
         if (accumulate && R != O) throw std::runtime_error("the accumulating tensor was not returned");
         std::memcpy(out, R->data().data(), sizeof(double) * o1 * o2);
+        return 0;
+    } catch (std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// coulombGrad (which 0) or exchangeGrad (which 1) through the functions above:
+// D1, D2 host (nao x nao) arrays (the same pointer: the same reference
+// Tensor), G host (natom x 3), accumulated.
+int shim_grad(int which, void* pl, int nterm, const double* scales, const double* omegas, const double* D1,
+              const double* D2, int D13symm, int D24symm, int Dsame, float thresp, float thredp, double* G)
+{
+    using namespace lightspeed;
+    try {
+        auto p = static_cast<oracle_ref::RefPairs*>(pl)->p;
+        auto ew = std::make_shared<Ewald>(std::vector<double>(scales, scales + nterm),
+                                          std::vector<double>(omegas, omegas + nterm));
+        auto res = ResourceList::build_cpu();
+        const size_t n = p->basis1()->nao(), natom = p->basis1()->natom();
+        auto A = std::make_shared<Tensor>(std::vector<size_t>{n, n});
+        std::memcpy(A->data().data(), D1, sizeof(double) * n * n);
+        std::shared_ptr<Tensor> B = A;
+        if (D2 != D1) {
+            B = std::make_shared<Tensor>(std::vector<size_t>{n, n});
+            std::memcpy(B->data().data(), D2, sizeof(double) * n * n);
+        }
+        auto Gt = std::make_shared<Tensor>(std::vector<size_t>{natom, 3});
+        std::memcpy(Gt->data().data(), G, sizeof(double) * natom * 3);
+        auto R = which ? b200::exchangeGrad(res, ew, p, A, B, D13symm != 0, D24symm != 0, Dsame != 0, thresp,
+                                            thredp, Gt)
+                       : b200::coulombGrad(res, ew, p, A, B, thresp, thredp, Gt);
+        if (R != Gt) throw std::runtime_error("the accumulating tensor was not returned");
+        std::memcpy(G, R->data().data(), sizeof(double) * natom * 3);
         return 0;
     } catch (std::exception& e) {
         g_err = e.what();

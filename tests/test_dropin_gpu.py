@@ -1,15 +1,17 @@
 """The drop-in boundary exercised from the reference's side.
 
 oracle/b200_shim.cpp is the binding a Lightspeed maintainer adds so that
-IntBox::coulomb / IntBox::exchange run on liblsjk.so: two functions with the
+IntBox::coulomb / IntBox::exchange (and the gradients coulombGrad /
+exchangeGrad) run on liblsjk.so: functions with the
 reference's signatures, written against the reference's own headers and
 types (Tensor, Basis, PairList, Ewald, ResourceList) and compiled from them
 (oracle/Makefile, target shim). These tests call them with reference Basis
 and PairList objects (built by the reference's own PairList::build_schwarz)
 and check the reference's golden vectors at the reference's tolerances
 (prop_int.py 1e-9, ewald_int.py and mix_basis.py 1e-12), the
-accumulate-into-J12 contract, and that a D24symm misuse raises the
-reference's error through the shim."""
+accumulate-into-J12 contract, that a D24symm misuse raises the
+reference's error through the shim, and the J/K nuclear gradients
+(coulombGrad / exchangeGrad) against the Jgr*/Kgr* goldens."""
 import ctypes
 import os
 
@@ -36,6 +38,7 @@ def shim():
     vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
     # typed arguments: an untyped Python int would go through as a 32-bit C int
     lib.shim_jk.argtypes = [ip, vp, vp, ip, vp, vp, vp, ip, fp, fp, ip, vp]
+    lib.shim_grad.argtypes = [ip, vp, ip, vp, vp, vp, vp, ip, ip, ip, fp, fp, vp]
     return lib
 
 
@@ -119,3 +122,35 @@ def test_d24symm_misuse_raises_reference_error(ls, shim):
     p11 = ref.RefPairs(b1, b1, True, 1e-14)
     with pytest.raises(RuntimeError, match="D24symm"):
         _jk(shim, 1, p12, p11, np.zeros((b2.nao, b1.nao)), symm=True)
+
+
+def _grad(shim, which, pl, D1, D2, flags=(1, 1, 1), thre=1e-14, G=None):
+    s = np.ascontiguousarray([1.0], np.float64)
+    o = np.ascontiguousarray([-1.0], np.float64)
+    A = np.ascontiguousarray(D1, np.float64)
+    B = A if D2 is None else np.ascontiguousarray(D2, np.float64)
+    natom = int(pl.b1.arrs["atom"][-1]) + 1
+    out = np.zeros((natom, 3)) if G is None else np.array(G, np.float64, copy=True)
+    rc = shim.shim_grad(which, pl.h, 1, _p(s), _p(o), _p(A), _p(B), flags[0], flags[1], flags[2],
+                        ctypes.c_float(thre), ctypes.c_float(thre), _p(out))
+    if rc:
+        raise RuntimeError(shim.shim_last_error().decode())
+    return out
+
+
+@pytest.mark.parametrize("basis", ["sto-3g", "6-31gs", "cc-pvdz"])
+def test_gradient_golden_through_reference_types(ls, shim, basis):
+    """coulombGrad / exchangeGrad with the reference's signatures and types
+    (the prop_int.py:142-211 calls) against its Jgr*/Kgr* golden vectors."""
+    z = np.load(os.path.join(ROOT, "tests", "golden", "ref_prop_h2o_%s.npz" % basis))
+    rb = _refbasis(ls, "h2o.xyz", basis)
+    pl = ref.RefPairs(rb, rb, True, 1e-14)
+    D, D2 = z["D"], z["D2"]
+    G = _grad(shim, 0, pl, D, None)
+    assert np.max(np.abs(G - z["Jgr"])) < 1e-9
+    assert np.max(np.abs(_grad(shim, 0, pl, D, None, G=G) - 2.0 * z["Jgr"])) < 2e-9
+    assert np.max(np.abs(_grad(shim, 0, pl, D, D2) - z["Jgr3"])) < 1e-9
+    assert np.max(np.abs(_grad(shim, 1, pl, D, None, (1, 1, 1)) - z["Kgr"])) < 1e-9
+    assert np.max(np.abs(_grad(shim, 1, pl, D2, None, (0, 0, 1)) - z["Kgr2"])) < 1e-9
+    assert np.max(np.abs(_grad(shim, 1, pl, D, D2, (1, 0, 0)) - z["Kgr3"])) < 1e-9
+    assert np.max(np.abs(_grad(shim, 1, pl, D2, D, (0, 1, 0)) - z["Kgr4"])) < 1e-9
