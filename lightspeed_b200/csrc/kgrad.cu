@@ -59,6 +59,12 @@ __device__ void kgrad_quartet(const KGradArgs& A, double alpha, double beta, dou
     constexpr int MA = L1 + L2 + 2, MC = L3 + L4 + 1;   // vertical-recursion extents (one quantum up)
     constexpr int XA = L1 + 2, XB = L2 + 2, XC = L3 + 2, XE = L4 + 1;
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
+    // light classes: every loop unrolled, so the 1-D integral tables live in
+    // registers with compile-time indices; the others keep runtime loops over
+    // local arrays (their tables are too large for registers)
+    constexpr bool kFlat = XA * XB * XC * XE <= 27 && N1 * N2 * N3 * N4 <= 27;
+    constexpr int U3 = kFlat ? 3 : 1, U1 = kFlat ? N1 : 1, U2 = kFlat ? N2 : 1, U3c = kFlat ? N3 : 1,
+                  U4 = kFlat ? N4 : 1, UR = kFlat ? NR : 1;
     double PQ[3], PA[3];
     double RR = 0.0;
 #pragma unroll
@@ -82,20 +88,23 @@ __device__ void kgrad_quartet(const KGradArgs& A, double alpha, double beta, dou
         }
         double t2[NR], w[NR];
         rys_eval<NR, double>(rho * d2 * RR, A.rys, A.nbin, A.tmax, A.asym_t, A.asym_w, t2, w);
-#pragma unroll 1
+#pragma unroll (UR)
         for (int r = 0; r < NR; ++r) {
             const double u = t2[r] * d2 * ipq;
             const double b00 = 0.5 * u, b10 = 0.5 * ip * (1.0 - q * u), b01 = 0.5 * iq * (1.0 - p * u);
             // 1-D integrals X[d][a][b][c][e], a <= L1+1, b <= L2+1, c <= L3+1, e <= L4
             // (the entries with a+b+c+e above L+1 are not exact for this rule and not used)
             double X[3][XA][XB][XC][XE];
-#pragma unroll 1
+#pragma unroll (U3)
             for (int d = 0; d < 3; ++d) {
                 const double c00 = PA[d] - q * u * PQ[d], d00 = QC[d] + p * u * PQ[d];
                 double I[MA + 1][MC + 1];
                 I[0][0] = d == 2 ? f * w[r] : 1.0;
+#pragma unroll
                 for (int a = 0; a < MA; ++a) I[a + 1][0] = c00 * I[a][0] + (a ? a * b10 * I[a - 1][0] : 0.0);
+#pragma unroll
                 for (int c = 0; c < MC; ++c)
+#pragma unroll
                     for (int a = 0; a <= MA; ++a) {
                         double v = d00 * I[a][c];
                         if (c) v += c * b01 * I[a][c - 1];
@@ -105,40 +114,54 @@ __device__ void kgrad_quartet(const KGradArgs& A, double alpha, double beta, dou
                 // transfer to centre 2, in place over a: H(a, b+1) = H(a+1, b) + (A - B) H(a, b);
                 // after step b, row a holds H(a, b) for a <= MA - b
                 double Hb[XB][XA][MC + 1];
+#pragma unroll
                 for (int a = 0; a < XA; ++a)
+#pragma unroll
                     for (int c = 0; c <= MC; ++c) Hb[0][a][c] = I[a][c];
+#pragma unroll
                 for (int b = 0; b + 1 < XB; ++b) {
+#pragma unroll
                     for (int a = 0; a + 1 <= MA - b; ++a)
+#pragma unroll
                         for (int c = 0; c <= MC; ++c) I[a][c] = I[a + 1][c] + Ar[d] * I[a][c];
+#pragma unroll
                     for (int a = 0; a < XA && a <= MA - b - 1; ++a)
+#pragma unroll
                         for (int c = 0; c <= MC; ++c) Hb[b + 1][a][c] = I[a][c];
                 }
                 // and to centre 4: (c, e+1) = (c+1, e) + (C - D) (c, e)
+#pragma unroll
                 for (int a = 0; a < XA; ++a)
+#pragma unroll
                     for (int b = 0; b < XB; ++b) {
                         if (a + b > MA) continue;
                         double Hd[MC + 1];
+#pragma unroll
                         for (int c = 0; c <= MC; ++c) Hd[c] = Hb[b][a][c];
+#pragma unroll
                         for (int c = 0; c < XC; ++c) X[d][a][b][c][0] = Hd[c];
+#pragma unroll
                         for (int e = 0; e + 1 < XE; ++e) {
+#pragma unroll
                             for (int c = 0; c + 1 <= MC - e; ++c) Hd[c] = Hd[c + 1] + Cr[d] * Hd[c];
+#pragma unroll
                             for (int c = 0; c < XC && c <= MC - e - 1; ++c) X[d][a][b][c][e + 1] = Hd[c];
                         }
                     }
             }
             // contraction with D13[i1, i3] D24[i2, i4]
-#pragma unroll 1
+#pragma unroll (U1)
             for (int i1 = 0; i1 < N1; ++i1) {
                 const int a[3] = {cart_lx(L1, i1), cart_ly(L1, i1), cart_lz(L1, i1)};
-#pragma unroll 1
+#pragma unroll (U3c)
                 for (int i3 = 0; i3 < N3; ++i3) {
                     const double d13 = D13[i1 * N3 + i3];
                     if (d13 == 0.0) continue;
                     const int c[3] = {cart_lx(L3, i3), cart_ly(L3, i3), cart_lz(L3, i3)};
-#pragma unroll 1
+#pragma unroll (U2)
                     for (int i2 = 0; i2 < N2; ++i2) {
                         const int b[3] = {cart_lx(L2, i2), cart_ly(L2, i2), cart_lz(L2, i2)};
-#pragma unroll 1
+#pragma unroll (U4)
                         for (int i4 = 0; i4 < N4; ++i4) {
                             const double W = d13 * D24[i2 * N4 + i4];
                             if (W == 0.0) continue;

@@ -4,8 +4,10 @@ reference CPU IntBox built from its sources, oracle/_ref).
 * C40H82 / cc-pVDZ (970 functions, 1290 primitive shells), Schwarz 1e-14, at
   the converged RHF density: J in FP64 elementwise within 1e-10 of the
   reference coulombCPU, and mixed-precision J (thredp = 1e-5) within 1e-6.
-  (The reference's K for this system takes tens of CPU minutes, so K is
-  checked on the shorter alkane below, whose quartets are the same kinds.)
+  K (FP64, merged-twin and mixed) against the reference's K through a
+  committed fixture (four K rows and the trace sum D K): the reference's K
+  for this system takes ~15 CPU minutes on 8 cores, so it is not recomputed
+  here.
 * C10H22 / cc-pVDZ at its converged density: J and symmetric K in FP64 within
   1e-10 of coulombCPU / exchangeCPU, and the mixed-precision build at the
   workload's thredp = 1e-5 within 1e-6 elementwise and |dE| <= 1e-6 Eh at fixed
@@ -182,4 +184,41 @@ def test_batched_k_vs_oracle(ls, ewald):
             Kr = ref.exchange(rp, rp, D, False, THRE, THRE, *ewald)
             assert np.max(np.abs(K.np - Kr)) < 1e-10
     finally:
+        ls.set_precision(ls.PREC_MIXED)
+
+
+def test_c40h82_k_vs_reference_fixture(ls, golden_dir):
+    """K of the full C40H82 / cc-pVDZ workload against the reference CPU
+    exchangeCPU, through a committed fixture (tests/golden/make_c40_kref.py: the
+    reference's K at a converged density): four K rows and the trace sum D K,
+    FP64 exact quartet set within 1e-10 (rows) and 1e-8 (trace); the
+    benchmark's merged-s-exponent K and mixed K beside it."""
+    import os
+    path = os.path.join(golden_dir, "c40h82_ccpvdz_kref.npz")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    from lightspeed_b200.geometry import alkane
+    z = np.load(path)
+    C = z["Cocc"]
+    D = C @ C.T
+    bas = ls.Basis.from_gbs_file(alkane(40), "cc-pvdz")
+    pl = ls.PairList.build_schwarz(bas, bas, True, THRE)
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    rows = list(z["rows"])
+    try:
+        ls.set_precision(ls.PREC_FP64)
+        K = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, THRE, THRE).np.copy()
+        assert np.max(np.abs(K[rows] - z["K_rows"])) < 1e-10
+        assert abs(float(np.sum(D * K)) - float(z["E_K"])) < 1e-8
+        ls.set_merge(True)
+        Km = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, THRE, THRE).np.copy()
+        assert np.max(np.abs(Km[rows] - z["K_rows"])) < 1e-9
+        ls.set_merge(False)
+        ls.set_precision(ls.PREC_MIXED)
+        Kx = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, THRE, THREDP).np.copy()
+        assert np.max(np.abs(Kx[rows] - z["K_rows"])) < 1e-6
+        assert abs(float(np.sum(D * Kx)) - float(z["E_K"])) < 1e-6
+    finally:
+        ls.set_merge(False)
         ls.set_precision(ls.PREC_MIXED)
