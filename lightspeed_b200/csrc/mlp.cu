@@ -4,9 +4,9 @@
 // weights updated by Adam. Entry points are declared in include/lsmlp.h; all
 // take device pointers and enqueue on the given stream.
 //
-// The network is tiny (three 256-wide layers, batches of a few thousand atom
-// pairs), so these are plain tiled SIMT kernels: 64 x 64 output tiles, 32-deep
-// K slices staged through shared memory and converted to FP32 on the load.
+// The products run on the tensor cores (BF16 mma.sync with FP32 accumulation,
+// 64 x 64 output tiles, 32-deep K slices staged through shared memory); the
+// element-wise kernels are plain grid-stride loops.
 #include <algorithm>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -24,59 +24,94 @@ int mlp_status(cudaError_t e)
     return 2;
 }
 
-constexpr int kTM = 64, kTN = 64, kTK = 32, kThreads = 256;
+constexpr int kTM = 64, kTN = 64, kTK = 32, kThreads = 128;
+constexpr int kPad = 8;   // bf16 elements of padding per shared-memory row
 
 // C[m][n] (+)= sum_k op(A)[m][k] op(B)[k][n]; op(A)[m][k] = ta ? A[k*lda+m] : A[m*lda+k],
 // op(B)[k][n] = tb ? B[n*ldb+k] : B[k*ldb+n].
+// BF16 tensor-core products with FP32 accumulation (mma.sync m16n8k16): a CTA
+// of four warps owns a 64 x 64 tile of C, each warp a 32 x 32 quarter as 2 x 4
+// fragments of 16 x 8; 32-deep K slices of op(A) (m-major rows) and op(B)
+// (n-major rows, i.e. k contiguous for the column operand) are staged in
+// shared memory as bf16, zero-filled past the matrix edges.
 __global__ void __launch_bounds__(kThreads)
 k_gemm_bf16(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
             int M, int N, int K, int lda, int ldb, int ldc, int ta, int tb, int accumulate)
 {
-    __shared__ float As[kTK][kTM + 1];
-    __shared__ float Bs[kTK][kTN + 1];
+    __shared__ __align__(16) __nv_bfloat16 As[kTM][kTK + kPad];
+    __shared__ __align__(16) __nv_bfloat16 Bs[kTN][kTK + kPad];
     const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;   // 16 x 16 threads, 4 x 4 outputs each
-    float acc[4][4] = {};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // the warp's quarter of the tile
+    const int grp = lane >> 2, tig = lane & 3;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+    float acc[2][4][4] = {};
     for (int k0 = 0; k0 < K; k0 += kTK) {
-        for (int idx = threadIdx.x; idx < kTK * kTM; idx += kThreads) {
-            const int kk = idx / kTM, mm = idx % kTM;
+        for (int idx = threadIdx.x; idx < kTM * kTK; idx += kThreads) {
+            const int mm = idx / kTK, kk = idx % kTK;
             const int m = m0 + mm, k = k0 + kk;
-            float v = 0.0f;
-            if (m < M && k < K) v = __bfloat162float(ta ? A[(long) k * lda + m] : A[(long) m * lda + k]);
-            As[kk][mm] = v;
+            __nv_bfloat16 v = zero;
+            if (m < M && k < K) v = ta ? A[(long) k * lda + m] : A[(long) m * lda + k];
+            As[mm][kk] = v;
         }
-        for (int idx = threadIdx.x; idx < kTK * kTN; idx += kThreads) {
-            const int kk = idx / kTN, nn = idx % kTN;
+        for (int idx = threadIdx.x; idx < kTN * kTK; idx += kThreads) {
+            const int nn = idx / kTK, kk = idx % kTK;
             const int n = n0 + nn, k = k0 + kk;
-            float v = 0.0f;
-            if (n < N && k < K) v = __bfloat162float(tb ? B[(long) n * ldb + k] : B[(long) k * ldb + n]);
-            Bs[kk][nn] = v;
+            __nv_bfloat16 v = zero;
+            if (n < N && k < K) v = tb ? B[(long) n * ldb + k] : B[(long) k * ldb + n];
+            Bs[nn][kk] = v;
         }
         __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < kTK; ++kk) {
-            float a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty + 16 * i];
+        for (int ks = 0; ks < kTK; ks += 16) {
+            // fragments (PTX mma.m16n8k16 layouts): A rows grp / grp + 8, k pairs tig*2 (+8);
+            // B column grp, k pairs tig*2 (+8)
+            unsigned a[2][4], b[4][2];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int mt = 0; mt < 2; ++mt) {
+                const int r = wm + mt * 16 + grp, c = ks + tig * 2;
+                a[mt][0] = *reinterpret_cast<const unsigned*>(&As[r][c]);
+                a[mt][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][c]);
+                a[mt][2] = *reinterpret_cast<const unsigned*>(&As[r][c + 8]);
+                a[mt][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][c + 8]);
+            }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int nt = 0; nt < 4; ++nt) {
+                const int r = wn + nt * 8 + grp, c = ks + tig * 2;
+                b[nt][0] = *reinterpret_cast<const unsigned*>(&Bs[r][c]);
+                b[nt][1] = *reinterpret_cast<const unsigned*>(&Bs[r][c + 8]);
+            }
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    float* d = acc[mt][nt];
+                    asm volatile(
+                        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+                        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                        : "r"(a[mt][0]), "r"(a[mt][1]), "r"(a[mt][2]), "r"(a[mt][3]), "r"(b[nt][0]),
+                          "r"(b[nt][1]));
+                }
         }
         __syncthreads();
     }
+    // accumulator layout: d0, d1 at row grp, columns tig*2, tig*2 + 1; d2, d3 at row grp + 8
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int m = m0 + ty + 16 * i, n = n0 + tx + 16 * j;
-            if (m < M && n < N) {
-                float* c = C + (long) m * ldc + n;
-                *c = accumulate ? *c + acc[i][j] : acc[i][j];
-            }
-        }
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int m = m0 + wm + mt * 16 + grp + 8 * h, n = n0 + wn + nt * 8 + tig * 2 + j;
+                    if (m < M && n < N) {
+                        float* c = C + (long) m * ldc + n;
+                        const float v = acc[mt][nt][2 * h + j];
+                        *c = accumulate ? *c + v : v;
+                    }
+                }
 }
 
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }

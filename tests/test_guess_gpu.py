@@ -3,8 +3,9 @@ the SAD guess, the local-frame block transforms, and a small end-to-end
 check that a network trained on converged densities starts the SCF closer to
 the answer than SAD and converges to the same energy.
 
-Tolerances: the BF16 GEMM is compared with float64 sums of the same bf16
-inputs at 1e-5 relative (FP32 accumulation of up to 256 terms); the
+Tolerances: the BF16 tensor-core GEMM is compared with float64 sums of the
+same bf16 inputs at 1e-5 relative (FP32 accumulation of up to 256 terms), in
+all four transposes and accumulating; the
 network's output and gradients at 2e-2 of their largest value, since an
 accumulation-order difference can flip one bf16 rounding of a hidden value."""
 import numpy as np
@@ -19,7 +20,7 @@ def _bf16_tensor(torch, a):
     return torch.tensor(mlp_ref.bf16(a), device="cuda").to(torch.bfloat16)
 
 
-@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1)])
+@pytest.mark.parametrize("ta,tb", [(0, 0), (1, 0), (0, 1), (1, 1)])
 def test_gemm_bf16_matches_float64(ls, ta, tb):
     import torch
     from lightspeed_b200.guess import _Lib, _p
@@ -36,6 +37,10 @@ def test_gemm_bf16_matches_float64(ls, ta, tb):
     k("lsmlp_gemm_bf16", _p(At), _p(Bt), _p(C), M, N, K, M if ta else K, K if tb else N, N, ta, tb, 0, None)
     torch.cuda.synchronize()
     assert np.max(np.abs(C.cpu().numpy() - ref)) <= 1e-5 * np.max(np.abs(ref))
+    # accumulate into C (the tensor-core tiles add to what is there)
+    k("lsmlp_gemm_bf16", _p(At), _p(Bt), _p(C), M, N, K, M if ta else K, K if tb else N, N, ta, tb, 1, None)
+    torch.cuda.synchronize()
+    assert np.max(np.abs(C.cpu().numpy() - 2.0 * ref)) <= 2e-5 * np.max(np.abs(ref))
 
 
 def test_mlp_forward_and_gradients_match_oracle(ls):
