@@ -11,15 +11,16 @@ namespace lsjk {
 
 
 
-// One J quartet (bra pair in registers, ket record r) accumulated into jp,
-// for the NG densities of the record (the Hermite integrals R_tuv are shared).
+// One J quartet (bra pair in registers, ket record r whose header q, Q the
+// caller has already loaded) accumulated into jp, for the NG densities of the
+// record (the Hermite integrals R_tuv are shared).
 template <int LB, int LK, int NG>
 __device__ __forceinline__ void j_quartet64(const JArgs& A, int g0, const double* tab, double p, double Px, double Py,
-                                            double Pz, const double* __restrict__ r, double (*jp)[nherm_of(LB)])
+                                            double Pz, double q, double Qx, double Qy, double Qz,
+                                            const double* __restrict__ r, double (*jp)[nherm_of(LB)])
 {
     constexpr int L = LB + LK, HK = nherm_of(LK);
-    const double q = r[0];
-    const double X = Px - r[1], Y = Py - r[2], Z = Pz - r[3];
+    const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;
     const double R2 = X * X + Y * Y + Z * Z;
     const double rs = rsqrt(p + q);
     const double rho = p * q * (rs * rs);
@@ -65,12 +66,12 @@ constexpr float kBoysSwitch32 = (float) (LSJK_BOYS_TMAX - LSJK_BOYS_TMAX / LSJK_
 // evaluated in FP64 by its asymptotic form), added to the FP64 accumulators.
 template <int LB, int LK, int NG>
 __device__ __forceinline__ void j_quartet32(const JArgs& A, int g0, const float* tab, float p,
-                                            double Px, double Py, double Pz, const double* __restrict__ r,
-                                            const float* __restrict__ r32, double (*jp)[nherm_of(LB)])
+                                            double Px, double Py, double Pz, double qd, double Qx, double Qy,
+                                            double Qz, const float* __restrict__ r32, double (*jp)[nherm_of(LB)])
 {
     constexpr int L = LB + LK, HB = nherm_of(LB), HK = nherm_of(LK);
-    const float q = r32[0];
-    const double Xd = Px - r[1], Yd = Py - r[2], Zd = Pz - r[3];
+    const float q = (float) qd;   // the FP32 record's q is this rounding
+    const double Xd = Px - Qx, Yd = Py - Qy, Zd = Pz - Qz;
     const float X = (float) Xd, Y = (float) Yd, Z = (float) Zd;
     const float R2 = X * X + Y * Y + Z * Z;
     const float rs = rsqrtf(p + q);
@@ -153,9 +154,29 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
     long nq = 0, nq32 = 0;
     const int nd = min(NG, A.ng - g0);   // statistics count density-quartets
     const int j1 = min(j0 + A.chunk, nk);
+    // the next ket's bound and record header are loaded one iteration ahead, so
+    // their latency overlaps the current quartet (all lanes read the same ket)
+    float Bn = A.kbound[j0];
+    double qn, Qxn, Qyn, Qzn;
+    {
+        const double* r = A.krec + (long) j0 * S;
+        qn = r[0];
+        Qxn = r[1];
+        Qyn = r[2];
+        Qzn = r[3];
+    }
     for (int j = j0; j < j1; ++j) {
-        const float Bj = A.kbound[j];
+        const float Bj = Bn;
+        const double qk = qn, Qx = Qxn, Qy = Qyn, Qz = Qzn;
         if (B0 * Bj < A.thresp) break;
+        if (j + 1 < j1) {
+            const double* rn = A.krec + (long) (j + 1) * S;
+            Bn = A.kbound[j + 1];
+            qn = rn[0];
+            Qxn = rn[1];
+            Qyn = rn[2];
+            Qzn = rn[3];
+        }
         const float est = Bi * Bj;
         const bool pass = act && est >= A.thresp;
         // one precision per warp and ket: FP64 while any lane's estimate reaches thredp
@@ -167,12 +188,13 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
         if (dp) {
             if (pass) {
                 nq += nd;
-                j_quartet64<LB, LK, NG>(A, g0, tab, p, Px, Py, Pz, r, jp);
+                j_quartet64<LB, LK, NG>(A, g0, tab, p, Px, Py, Pz, qk, Qx, Qy, Qz, r, jp);
             }
         } else if (__any_sync(0xffffffffu, pass)) {
             if (pass) {
                 nq32 += nd;
-                j_quartet32<LB, LK, NG>(A, g0, tab32, p32, Px, Py, Pz, r, A.krec32 + (long) j * S, jp);
+                j_quartet32<LB, LK, NG>(A, g0, tab32, p32, Px, Py, Pz, qk, Qx, Qy, Qz, A.krec32 + (long) j * S,
+                                        jp);
             }
         }
     }

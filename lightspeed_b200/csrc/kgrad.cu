@@ -27,6 +27,7 @@ namespace lsjk {
 namespace {
 
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
+constexpr int kGradWarpMin = 324;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).
 __device__ __forceinline__ float grad_threshold(double thr, double dmax)
@@ -46,6 +47,24 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// Light classes (small 1-D integral tables and few Cartesian combinations):
+// one lane per quartet with every loop unrolled into registers.
+template <int L1, int L2, int L3, int L4>
+__host__ __device__ constexpr bool kgrad_flat()
+{
+    return (L1 + 2) * (L2 + 2) * (L3 + 2) * (L4 + 1) <= 27 &&
+           ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) <= 27;
+}
+
+// The heaviest classes (at least 324 Cartesian combinations: (dd|pp), (dp|dp)
+// and above) run one quartet per warp with the tables in shared memory; the
+// rest one quartet per lane.
+template <int L1, int L2, int L3, int L4>
+__host__ __device__ constexpr bool kgrad_warp()
+{
+    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin;
+}
+
 // One quartet's derivatives at centres 1, 2 and 3 contracted with the D13 and
 // D24 blocks, added into gA, gB, gC.
 template <int L1, int L2, int L3, int L4>
@@ -62,7 +81,7 @@ __device__ void kgrad_quartet(const KGradArgs& A, double alpha, double beta, dou
     // light classes: every loop unrolled, so the 1-D integral tables live in
     // registers with compile-time indices; the others keep runtime loops over
     // local arrays (their tables are too large for registers)
-    constexpr bool kFlat = XA * XB * XC * XE <= 27 && N1 * N2 * N3 * N4 <= 27;
+    constexpr bool kFlat = kgrad_flat<L1, L2, L3, L4>();
     constexpr int U3 = kFlat ? 3 : 1, U1 = kFlat ? N1 : 1, U2 = kFlat ? N2 : 1, U3c = kFlat ? N3 : 1,
                   U4 = kFlat ? N4 : 1, UR = kFlat ? NR : 1;
     double PQ[3], PA[3];
@@ -308,11 +327,249 @@ __global__ void __launch_bounds__(128) k_exchange_grad(const __grid_constant__ K
     }
 }
 
+// Per-warp shared tables of the warp-cooperative quartet.
+template <int L1, int L2, int L3, int L4>
+struct KGradWarpTables {
+    static constexpr int MA = L1 + L2 + 2, MC = L3 + L4 + 1, XA = L1 + 2, XB = L2 + 2, XC = L3 + 2, XE = L4 + 1;
+    double X[3][XA][XB][XC][XE];      // 1-D integrals (as in kgrad_quartet)
+    double I[3][MA + 1][MC + 1];      // vertical recursion, per direction
+    double Hb[3][XB][XA][MC + 1];     // after the transfer to centre 2
+    double D13[ncart_of(L1) * ncart_of(L3)];
+    double D24[ncart_of(L2) * ncart_of(L4)];
+};
+
+// One quartet of a heavy class, computed by the whole warp: lanes 0-2 run the
+// vertical recursion and the transfer to centre 2 of one direction each, the
+// lanes share the transfers to centre 4 (one (direction, a, b) row each) and
+// the Cartesian combinations of the contraction; the tables live in shared
+// memory. Each lane returns its part of the derivative sums.
+template <int L1, int L2, int L3, int L4>
+__device__ void kgrad_quartet_warp(const KGradArgs& A, KGradWarpTables<L1, L2, L3, L4>& S, int lane, double alpha,
+                                   double beta, double gamma, double kab12, double p, double ip, const double P[3],
+                                   const double Ar[3], double kab34, double q, double iq, const double Qs[3],
+                                   const double QC[3], const double Cr[3], double gA[3], double gB[3], double gC[3])
+{
+    using Tab = KGradWarpTables<L1, L2, L3, L4>;
+    constexpr int NR = (L1 + L2 + L3 + L4 + 1) / 2 + 1;
+    constexpr int MA = Tab::MA, MC = Tab::MC, XA = Tab::XA, XB = Tab::XB, XC = Tab::XC, XE = Tab::XE;
+    constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
+    constexpr int NC = N1 * N3 * N2 * N4;
+    double PQ[3], PA[3];
+    double RR = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        PQ[d] = P[d] + Qs[d];
+        PA[d] = P[d] - Ar[d];
+        RR += PQ[d] * PQ[d];
+    }
+    const double rs = rsqrt(p + q);
+    const double ipq = rs * rs;
+    const double rho = p * q * ipq;
+    const double pref = kTwoPi52G * (kab12 * kab34) * rs;
+    // this lane's direction in the recursions (lanes 0-2)
+    const int dl = lane < 3 ? lane : 0;
+    const double PAd = dl == 0 ? PA[0] : (dl == 1 ? PA[1] : PA[2]);
+    const double PQd = dl == 0 ? PQ[0] : (dl == 1 ? PQ[1] : PQ[2]);
+    const double QCd = dl == 0 ? QC[0] : (dl == 1 ? QC[1] : QC[2]);
+    const double ABd = dl == 0 ? Ar[0] : (dl == 1 ? Ar[1] : Ar[2]);
+#pragma unroll 1
+    for (int tm = 0; tm < A.nterm; ++tm) {
+        double d2 = 1.0, f = A.alpha[tm] * pref;
+        if (A.omega[tm] != -1.0) {
+            const double w2 = A.omega[tm] * A.omega[tm];
+            d2 = w2 / (rho + w2);
+            f *= sqrt(d2);
+        }
+        double t2[NR], w[NR];
+        rys_eval<NR, double>(rho * d2 * RR, A.rys, A.nbin, A.tmax, A.asym_t, A.asym_w, t2, w);
+#pragma unroll 1
+        for (int r = 0; r < NR; ++r) {
+            const double u = t2[r] * d2 * ipq;
+            const double b00 = 0.5 * u, b10 = 0.5 * ip * (1.0 - q * u), b01 = 0.5 * iq * (1.0 - p * u);
+            if (lane < 3) {
+                // vertical recursion and transfer to centre 2 of direction dl
+                double (*I)[MC + 1] = S.I[dl];
+                const double c00 = PAd - q * u * PQd, d00 = QCd + p * u * PQd;
+                I[0][0] = dl == 2 ? f * w[r] : 1.0;
+#pragma unroll
+                for (int a = 0; a < MA; ++a) I[a + 1][0] = c00 * I[a][0] + (a ? a * b10 * I[a - 1][0] : 0.0);
+#pragma unroll
+                for (int c = 0; c < MC; ++c)
+#pragma unroll
+                    for (int a = 0; a <= MA; ++a) {
+                        double v = d00 * I[a][c];
+                        if (c) v += c * b01 * I[a][c - 1];
+                        if (a) v += a * b00 * I[a - 1][c];
+                        I[a][c + 1] = v;
+                    }
+#pragma unroll
+                for (int a = 0; a < XA; ++a)
+#pragma unroll
+                    for (int c = 0; c <= MC; ++c) S.Hb[dl][0][a][c] = I[a][c];
+#pragma unroll
+                for (int b = 0; b + 1 < XB; ++b) {
+#pragma unroll
+                    for (int a = 0; a + 1 <= MA - b; ++a)
+#pragma unroll
+                        for (int c = 0; c <= MC; ++c) I[a][c] = I[a + 1][c] + ABd * I[a][c];
+#pragma unroll
+                    for (int a = 0; a < XA && a <= MA - b - 1; ++a)
+#pragma unroll
+                        for (int c = 0; c <= MC; ++c) S.Hb[dl][b + 1][a][c] = I[a][c];
+                }
+            }
+            __syncwarp();
+            // transfers to centre 4, one (direction, a, b) row per lane
+            for (int job = lane; job < 3 * XA * XB; job += 32) {
+                const int d = job / (XA * XB), a = (job / XB) % XA, b = job % XB;
+                if (a + b > MA) continue;
+                const double CD = d == 0 ? Cr[0] : (d == 1 ? Cr[1] : Cr[2]);
+                double Hd[MC + 1];
+#pragma unroll
+                for (int c = 0; c <= MC; ++c) Hd[c] = S.Hb[d][b][a][c];
+#pragma unroll
+                for (int c = 0; c < XC; ++c) S.X[d][a][b][c][0] = Hd[c];
+#pragma unroll
+                for (int e = 0; e + 1 < XE; ++e) {
+#pragma unroll
+                    for (int c = 0; c + 1 <= MC - e; ++c) Hd[c] = Hd[c + 1] + CD * Hd[c];
+#pragma unroll
+                    for (int c = 0; c < XC && c <= MC - e - 1; ++c) S.X[d][a][b][c][e + 1] = Hd[c];
+                }
+            }
+            __syncwarp();
+            // the Cartesian combinations (i1, i3, i2, i4) over the lanes
+            for (int cmb = lane; cmb < NC; cmb += 32) {
+                const int i4 = cmb % N4, i2 = (cmb / N4) % N2, i13 = cmb / (N4 * N2);
+                const int i1 = i13 / N3, i3 = i13 % N3;
+                const double W = S.D13[i1 * N3 + i3] * S.D24[i2 * N4 + i4];
+                if (W == 0.0) continue;
+                const int a[3] = {cart_lx(L1, i1), cart_ly(L1, i1), cart_lz(L1, i1)};
+                const int b[3] = {cart_lx(L2, i2), cart_ly(L2, i2), cart_lz(L2, i2)};
+                const int c[3] = {cart_lx(L3, i3), cart_ly(L3, i3), cart_lz(L3, i3)};
+                const int e[3] = {cart_lx(L4, i4), cart_ly(L4, i4), cart_lz(L4, i4)};
+                double v[3], da[3], db[3], dc[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int ad = a[d], bd = b[d], cd = c[d], ed = e[d];
+                    v[d] = S.X[d][ad][bd][cd][ed];
+                    da[d] = 2.0 * alpha * S.X[d][ad + 1][bd][cd][ed];
+                    if (ad) da[d] -= ad * S.X[d][ad - 1][bd][cd][ed];
+                    db[d] = 2.0 * beta * S.X[d][ad][bd + 1][cd][ed];
+                    if (bd) db[d] -= bd * S.X[d][ad][bd - 1][cd][ed];
+                    dc[d] = 2.0 * gamma * S.X[d][ad][bd][cd + 1][ed];
+                    if (cd) dc[d] -= cd * S.X[d][ad][bd][cd - 1][ed];
+                }
+                const double yz = W * v[1] * v[2], xz = W * v[0] * v[2], xy = W * v[0] * v[1];
+                gA[0] += da[0] * yz;
+                gA[1] += da[1] * xz;
+                gA[2] += da[2] * xy;
+                gB[0] += db[0] * yz;
+                gB[1] += db[1] * xz;
+                gB[2] += db[2] * xy;
+                gC[0] += dc[0] * yz;
+                gC[1] += dc[1] * xz;
+                gC[2] += dc[2] * xy;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Heavy classes: the warp walks the task's passing (partner 1, partner 3)
+// quartets one at a time (partners 3 outer, both rows in bound order, the same
+// screens as k_exchange_grad) and computes each with kgrad_quartet_warp.
+template <int L1, int L2, int L3, int L4>
+__global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constant__ KGradArgs A)
+{
+    constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
+    __shared__ KGradWarpTables<L1, L2, L3, L4> tabs[4];
+    KGradWarpTables<L1, L2, L3, L4>& S = tabs[threadIdx.x >> 5];
+    const int ntask = *A.ntask;
+    const int lane = threadIdx.x & 31;
+    const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = (int) atomicAdd(A.queue, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= ntask) break;
+        const KTask T = A.tasks[t];
+        const int i2 = T.i2, i4 = T.i4;
+        const float tlo = grad_threshold((double) A.thr_lo, T.dmax);
+        const double dR[3] = {A.b2.x[i2] - A.b4.x[i4], A.b2.y[i2] - A.b4.y[i4], A.b2.z[i2] - A.b4.z[i4]};
+        const double beta = A.b2.e[i2];
+        const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
+        __syncwarp();   // the previous task's tables have been read
+        for (int idx = lane; idx < N2 * N4; idx += 32)
+            S.D24[idx] = A.D24[(long) (c2 + idx / N4) * A.ld24 + c4 + idx % N4];
+        const int s12 = A.r12s[i2], n12 = A.r12l[i2], s34 = A.r34s[i4], n34 = A.r34l[i4];
+        const float b12max = A.b12[s12];
+        double gB[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
+        for (int k = 0; k < n34; ++k) {
+            const int k3 = s34 + k;
+            const float b34 = A.b34[k3];
+            if (b34 < thre34 || b12max * b34 < tlo) break;   // bound order: nothing later passes
+            const double kab34 = A.kab34[k3], q = A.p34[k3], iq = A.ip34[k3], gamma = A.pe34[k3];
+            const double Q[3] = {A.px34[k3], A.py34[k3], A.pz34[k3]};
+            const double Cr[3] = {A.ax34[k3], A.ay34[k3], A.az34[k3]};
+            double QC[3], Qs[3];
+            for (int d = 0; d < 3; ++d) {
+                QC[d] = Q[d] - Cr[d];
+                Qs[d] = dR[d] - Q[d];
+            }
+            const int c3 = A.cart34[k3], atomC = A.atom34[k3], K3 = A.pidx34[k3];
+            double gC[3] = {0, 0, 0};
+            for (int j = 0; j < n12; ++j) {
+                const int e = s12 + j;
+                const float b12 = A.b12[e];
+                if (b12 < thre12 || b12 * b34 < tlo) break;
+                if (A.canon) {
+                    const int K1 = A.pidx12[e];
+                    const int r2 = K1 > i2 ? K1 : i2, r4 = K3 > i4 ? K3 : i4;
+                    if ((double) (b12 * b34) * A.dblk[(long) r2 * A.nprim + r4] < (double) A.thr_lo) continue;
+                }
+                const double P[3] = {A.px12[e], A.py12[e], A.pz12[e]};
+                const double Ar[3] = {A.ax12[e], A.ay12[e], A.az12[e]};
+                const int c1 = A.cart12[e];
+                __syncwarp();   // the previous quartet's D13 has been read
+                for (int idx = lane; idx < N1 * N3; idx += 32)
+                    S.D13[idx] = A.D13[(long) (c1 + idx / N3) * A.ld13 + c3 + idx % N3];
+                __syncwarp();
+                double qa[3] = {0, 0, 0}, qb[3] = {0, 0, 0}, qc[3] = {0, 0, 0};
+                kgrad_quartet_warp<L1, L2, L3, L4>(A, S, lane, A.pe12[e], beta, gamma, A.kab12[e], A.p12[e],
+                                                   A.ip12[e], P, Ar, kab34, q, iq, Qs, QC, Cr, qa, qb, qc);
+                const int atomA = A.atom12[e];
+                for (int d = 0; d < 3; ++d) {
+                    const double sa = warp_sum(qa[d]);
+                    if (lane == 0 && sa != 0.0) atomicAdd(&A.G[3 * atomA + d], sa);
+                    gB[d] += qb[d];
+                    gC[d] += qc[d];
+                    gD[d] -= qa[d] + qb[d] + qc[d];   // translational invariance
+                }
+            }
+            for (int d = 0; d < 3; ++d) {
+                const double sc = warp_sum(gC[d]);
+                if (lane == 0 && sc != 0.0) atomicAdd(&A.G[3 * atomC + d], sc);
+            }
+        }
+        for (int d = 0; d < 3; ++d) {
+            const double sb = warp_sum(gB[d]), sd = warp_sum(gD[d]);
+            if (lane == 0) {
+                if (sb != 0.0) atomicAdd(&A.G[3 * A.b2.atom[i2] + d], sb);
+                if (sd != 0.0) atomicAdd(&A.G[3 * A.b4.atom[i4] + d], sd);
+            }
+        }
+    }
+}
+
 template <int L1, int L2, int L3, int L4>
 void launch_one(Context* ctx, const KGradArgs& A, long cap)
 {
     const unsigned grid = (unsigned) std::min<long>((cap + 3) / 4, (long) ctx->nsm * 8);
-    k_exchange_grad<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
+    if constexpr (kgrad_warp<L1, L2, L3, L4>())
+        k_exchange_grad_warp<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
+    else
+        k_exchange_grad<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
 }
