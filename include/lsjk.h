@@ -258,8 +258,11 @@ int lsjk_potential(lsjk_context* ctx, int nterm, const double* scales, const dou
  * G (natom x 3, row-major, host) += sum_{pqrs} D13_pr d(pq|rs)/dR D24_qs over a
  * symmetric pair list; D13, D24 are host nao x nao matrices. D13symm, D24symm
  * and Dsame are the reference's promises (symmetric D13, symmetric D24, D13 ==
- * D24): they select which equal terms the reference skips and doubles, so the
- * sum does not depend on them here and every quartet is computed. FP64
+ * D24): with D13symm and D24symm the engine computes each pair of equal terms
+ * (12|34), (34|12) once and doubles it; all three select the reference's fully
+ * symmetric routine, whose screen (and result near thresp) the engine
+ * reproduces, reading D13 alone. A false promise gives a wrong gradient, as in
+ * the reference. FP64
  * throughout (thredp is ignored, as on the reference's CPU path); quartets
  * screened like K (B_12 B_34 max|D24 block| >= thresp). LSJK_EINVAL for a
  * non-symmetric list. */

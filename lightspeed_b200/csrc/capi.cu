@@ -817,7 +817,7 @@ int lsjk_exchange_grad(lsjk_context* ctx, int nterm, const double* scales, const
         double* D24c = same ? D13c : lsjk::take<double>(c, (size_t) b->ncart * b->ncart);
         lsjk::pure_to_cart(c, b, b, dD, D13c);
         if (!same) lsjk::pure_to_cart(c, b, b, dD + nD, D24c);
-        lsjk::exchange_grad(c, ew, p, D13c, D24c, canon, dG, thresp);
+        lsjk::exchange_grad(c, ew, p, D13c, D24c, D13symm && D24symm, canon, dG, thresp);
         LSJK_CUDA(cudaMemcpyAsync(h, dG, sizeof(double) * nG, cudaMemcpyDeviceToHost, c->stream));
         check_kernels(c);
         for (size_t i = 0; i < nG; ++i) G[i] += h[i];

@@ -353,9 +353,10 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     bool d24symm, bool flip_ok, float thresp, float thredp, const Basis* kb1, const Basis* kb3);
 // K nuclear gradient (FP64): G[atom][xyz] += sum D13 d(12|34)/dR D24 over the
 // K-invert quartets of a symmetric pair list (K-invert rows built), Cartesian
-// densities in, device G (natom x 3) accumulated. canon: the quartet screen of
-// the reference's fully symmetric routine (D13 == D24 symmetric).
+// densities in, device G (natom x 3) accumulated. pairsym: D13 and D24 are both
+// symmetric (each term computed once for itself and its mirror); canon: the
+// quartet screen of the reference's fully symmetric routine (D13 == D24 symmetric).
 void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D13cart, const double* D24cart,
-                   bool canon, double* G, float thresp);
+                   bool pairsym, bool canon, double* G, float thresp);
 
 } // namespace lsjk

@@ -217,7 +217,8 @@ public:
                                                const std::shared_ptr<Tensor>& G = std::shared_ptr<Tensor>());
     // K nuclear gradient (src/lightspeed/intbox.hpp:1095-1160): G (natom, 3) +=
     // sum D13 d(12|34) D24 over a symmetric pair list. D13symm, D24symm, Dsame
-    // are accepted as the reference's promises; the sum does not depend on them.
+    // are the reference's promises: D13symm and D24symm let each pair of equal terms
+    // be computed once; all three select the reference's fully symmetric routine.
     static std::shared_ptr<Tensor> exchangeGrad(const std::shared_ptr<ResourceList>& resources,
                                                 const std::shared_ptr<Ewald>& ewald,
                                                 const std::shared_ptr<PairList>& pairlist,

@@ -115,6 +115,10 @@ struct KGradArgs {
     const double* dblk;
     int nprim;
     int canon;
+    // pairsym != 0 (D13 and D24 both symmetric): the tasks have prim2 <= prim4 and
+    // a task with prim2 < prim4 stands for itself and its mirror (1,2,3,4) <-> (3,4,1,2),
+    // whose terms are equal: its D24 block enters doubled
+    int pairsym;
     const double* rys;          // FP64 Rys table block of the rule one quantum up
     const double* asym_t;
     const double* asym_w;

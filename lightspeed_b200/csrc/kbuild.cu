@@ -466,9 +466,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
 // the reference's fully symmetric routine (D13symm, D24symm and Dsame;
 // exchange_grad.cpp:17-470), which computes one representative per set of
 // equal terms and screens all of them with the representative's D block;
-// the same sum over the same quartets here.
+// the same sum over the same quartets here. `pairsym` (D13 and D24 both
+// symmetric, the reference's D13symm and D24symm): the terms of (1,2,3,4) and
+// (3,4,1,2) are equal, screens included, so only tasks with prim2 <= prim4 run
+// and those with prim2 < prim4 count twice.
 void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const double* D13cart, const double* D24cart,
-                   bool canon, double* G, float thresp)
+                   bool pairsym, bool canon, double* G, float thresp)
 {
     if (ew.alpha.size() > 4) throw Error(LSJK_EINVAL, "exchange_grad: at most 4 Ewald terms");
     cudaStream_t s = ctx->stream;
@@ -508,7 +511,7 @@ void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const doub
     T.Dc[0] = D24cart;
     T.ng = 1;
     T.ld4 = b->ncart;
-    T.d24symm = 0;
+    T.d24symm = pairsym ? 1 : 0;   // prim2 <= prim4 when each task also stands for its mirror
     T.thresp = thresp;
     T.sc = sc;
     T.tasks = tasks;
@@ -562,6 +565,7 @@ void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const doub
                     A.dblk = dblk;
                     A.nprim = b->nprim;
                     A.canon = canon ? 1 : 0;
+                    A.pairsym = pairsym ? 1 : 0;
                     A.b2 = A.b4 = b->view();
                     A.D13 = D13cart;
                     A.ld13 = b->ncart;

@@ -233,9 +233,10 @@ __global__ void __launch_bounds__(128) k_exchange_grad(const __grid_constant__ K
         const double dR[3] = {A.b2.x[i2] - A.b4.x[i4], A.b2.y[i2] - A.b4.y[i4], A.b2.z[i2] - A.b4.z[i4]};
         const double beta = A.b2.e[i2];
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
+        const double w24 = (A.pairsym && i2 != i4) ? 2.0 : 1.0;   // a task and its mirror
         double D24[N2 * N4];
         for (int a = 0; a < N2; ++a)
-            for (int b = 0; b < N4; ++b) D24[a * N4 + b] = A.D24[(long) (c2 + a) * A.ld24 + c4 + b];
+            for (int b = 0; b < N4; ++b) D24[a * N4 + b] = w24 * A.D24[(long) (c2 + a) * A.ld24 + c4 + b];
         const int s12 = A.r12s[i2], n12 = A.r12l[i2], s34 = A.r34s[i4], n34 = A.r34l[i4];
         double gB[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
         for (int cs = 0; cs < n34; cs += 32) {
@@ -499,9 +500,10 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
         const double dR[3] = {A.b2.x[i2] - A.b4.x[i4], A.b2.y[i2] - A.b4.y[i4], A.b2.z[i2] - A.b4.z[i4]};
         const double beta = A.b2.e[i2];
         const int c2 = A.b2.cart[i2], c4 = A.b4.cart[i4];
+        const double w24 = (A.pairsym && i2 != i4) ? 2.0 : 1.0;   // a task and its mirror
         __syncwarp();   // the previous task's tables have been read
         for (int idx = lane; idx < N2 * N4; idx += 32)
-            S.D24[idx] = A.D24[(long) (c2 + idx / N4) * A.ld24 + c4 + idx % N4];
+            S.D24[idx] = w24 * A.D24[(long) (c2 + idx / N4) * A.ld24 + c4 + idx % N4];
         const int s12 = A.r12s[i2], n12 = A.r12l[i2], s34 = A.r34s[i4], n34 = A.r34l[i4];
         const float b12max = A.b12[s12];
         double gB[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
