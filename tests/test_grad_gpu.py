@@ -152,6 +152,9 @@ def test_exchange_grad_vs_oracle(ls, case):
     assert np.max(np.abs(G_same - Gr_same)) < 1e-9
     assert np.max(np.abs(G_ab - Gr_ab)) < 1e-9
     assert np.max(np.abs(G_ab.sum(axis=0))) < 1e-9
+    # without the symmetry promises every ordered quartet runs (no mirror halving): same sum
+    G_nosym = ls.IntBox.exchangeGrad(res, ew, pl, A, B, False, False, False, thre, thre).np
+    assert np.max(np.abs(G_nosym - Gr_ab)) < 1e-9
 
 
 def test_exchange_grad_range_separated(ls, golden_dir):
