@@ -98,8 +98,15 @@ int lsjk_context_set_merge(lsjk_context* ctx, int on);
 void* lsjk_context_stream(lsjk_context* ctx);
 int lsjk_context_stats(lsjk_context* ctx, lsjk_stats* out);
 int lsjk_context_reset_stats(lsjk_context* ctx);
-/* Raw per-class quartet counters: [precision FP64, FP32][J classes (LB*5+LK),
- * K classes ((L1*3+L2)*3+L3)*3+L4]; n must be >= 2*(25+81). */
+/* Largest shell the kernels take (f) and the class counts it gives: J classes
+ * (LB, LK) with Hermite orders LB, LK = 0..2 LSJK_LMAX, K classes (L1,L2,L3,L4)
+ * with L = 0..LSJK_LMAX. */
+#define LSJK_LMAX 3
+#define LSJK_NJCLASS ((2 * LSJK_LMAX + 1) * (2 * LSJK_LMAX + 1))
+#define LSJK_NKCLASS ((LSJK_LMAX + 1) * (LSJK_LMAX + 1) * (LSJK_LMAX + 1) * (LSJK_LMAX + 1))
+/* Raw per-class quartet counters: [precision FP64, FP32][J classes
+ * LB*(2 LSJK_LMAX+1)+LK, K classes ((L1*n+L2)*n+L3)*n+L4 with n = LSJK_LMAX+1];
+ * n must be >= 2*(LSJK_NJCLASS+LSJK_NKCLASS). */
 int lsjk_context_counters(lsjk_context* ctx, unsigned long long* out, int n);
 /* Algorithmic flops of the quartets counted since the last reset, split by
  * precision: out[0] J in FP64, out[1] J in FP32, out[2] K in FP64, out[3] K
@@ -114,7 +121,7 @@ int lsjk_context_flops_split(lsjk_context* ctx, double* out4);
  * then use the table. The table (LSJK_TUNE_INTS ints: J chunk per (LB,LK),
  * then K CTAs/SM per pass and class; 0 = default) can be saved and restored
  * (set = 0: read, 1: write) so a workload is tuned once. */
-#define LSJK_TUNE_INTS (25 + 2 * 81)
+#define LSJK_TUNE_INTS (LSJK_NJCLASS + 2 * LSJK_NKCLASS)
 int lsjk_context_set_autotune(lsjk_context* ctx, int on);
 int lsjk_context_tune_table(lsjk_context* ctx, int* table, int n, int set);
 /* Copy the device status word of the context's kernels (0 = no error). */

@@ -30,7 +30,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 LIB = os.path.join(PKG, "liblsjk.so")
-LMAX = 2
+LMAX = 3        # largest shell of the kernels (f)
+GEN_LMAX = 2    # largest shell of the straight-line quartet code; above it the loop form
 
 
 def _mtime(p):
@@ -57,14 +58,17 @@ def gen_sources(force=False):
     kgen = os.path.join(CSRC, "gen_kernels.py")
     jq = os.path.join(CSRC, "generated", "jquartets.cuh")
     if force or _mtime(jq) < _mtime(kgen):
-        _run([sys.executable, kgen, str(LMAX)], cwd=ROOT)
+        _run([sys.executable, kgen, str(GEN_LMAX)], cwd=ROOT)
 
 
 def cuda_units():
     """(object name, source, extra flags) for every translation unit."""
     units = []
-    for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "kgrad", "oneint", "mlp"):
+    for name in ("basis", "pairs", "capi", "jbuild", "kbuild", "oneint", "mlp"):
         units.append((name, os.path.join(CSRC, name + ".cu"), []))
+    # K gradient classes, one unit per partner-1 shell
+    for l1 in range(LMAX + 1):
+        units.append(("kgrad_%d" % l1, os.path.join(CSRC, "kgrad.cu"), ["-DLSJK_KG_L1=%d" % l1]))
     # bra Hermite classes 0..2*LMAX, and 2*LMAX+1 for the gradients
     for lb in range(2 * LMAX + 2):
         units.append(("jinst_%d" % lb, os.path.join(CSRC, "jinst.cu"), ["-DLSJK_LB=%d" % lb]))

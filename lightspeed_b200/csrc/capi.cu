@@ -106,7 +106,7 @@ void check_kernels(lsjk::Context* ctx)
 void check_lmax(const lsjk::PairList* pl)
 {
     if (pl->b1->maxL > lsjk::kLmax || pl->b2->maxL > lsjk::kLmax)
-        throw lsjk::Error(LSJK_ENOTSUPP, "J/K: angular momentum above d is not supported by the GPU kernels");
+        throw lsjk::Error(LSJK_ENOTSUPP, "J/K: angular momentum above f is not supported by the GPU kernels");
 }
 
 // The pair list a K build runs over: its merged twin (shared s exponents of a

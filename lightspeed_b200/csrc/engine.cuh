@@ -25,9 +25,9 @@
 
 namespace lsjk {
 
-constexpr int kLmax = 2;                       // s, p, d shells (generated kernels)
+constexpr int kLmax = LSJK_LMAX;               // s, p, d, f shells
 constexpr int kNL = kLmax + 1;
-constexpr int kNHerm = 2 * kLmax + 1;          // Hermite classes L1+L2 = 0..4
+constexpr int kNHerm = 2 * kLmax + 1;          // Hermite classes L1+L2 = 0..6
 
 inline int ncart_count(int L) { return (L + 1) * (L + 2) / 2; }
 
@@ -35,6 +35,7 @@ inline int ncart_count(int L) { return (L + 1) * (L + 2) / 2; }
 constexpr int kNJClass = kNHerm * kNHerm;            // (LB, LK)
 constexpr int kNKClass = kNL * kNL * kNL * kNL;      // (L1, L2, L3, L4)
 constexpr int kNCounters = 2 * (kNJClass + kNKClass); // [prec][J classes, K classes]
+static_assert(kNJClass == LSJK_NJCLASS && kNKClass == LSJK_NKCLASS, "class counts of the C ABI");
 
 struct Error : std::runtime_error {
     int code;

@@ -238,7 +238,9 @@ def main():
     for LB in range(2 * lmax + 2):
         for LK in range(2 * lmax + 1):
             jparts.append(gen_j(LB, LK))
-    jparts.append("template <int LB, int LK> struct JQ;")
+    # classes not emitted here (shells above LMAX) take the loop form
+    jparts.append('#include "quartet_loops.cuh"')
+    jparts.append("template <int LB, int LK> struct JQ : lsjk::JQLoop<LB, LK> {};")
     for LB in range(2 * lmax + 2):
         for LK in range(2 * lmax + 1):
             jparts.append("template <> struct JQ<%d, %d> { template <typename R> __device__ __forceinline__ static void "
@@ -253,7 +255,8 @@ def main():
             "R cdx, R cdy, R cdz, R wz, const R* D, R* K")
     call = "c00x, c00y, c00z, d00x, d00y, d00z, b00, b10, b01, abx, aby, abz, cdx, cdy, cdz, wz, D, K"
     kfwd = list(head)
-    kfwd.append("template <int L1, int L2, int L3, int L4> struct KQ;")
+    kfwd.append('#include "quartet_loops.cuh"')
+    kfwd.append("template <int L1, int L2, int L3, int L4> struct KQ : lsjk::KQLoop<L1, L2, L3, L4> {};")
     kfwd.append("template <int L1, int L2, int L3, int L4, typename R> __device__ __forceinline__ void kq_dispatch(%s) "
                 "{ KQ<L1, L2, L3, L4>::run(%s); }" % (args, call))
     with open(os.path.join(out_dir, "kquartets_fwd.cuh"), "w") as fh:

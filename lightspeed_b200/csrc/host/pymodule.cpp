@@ -223,17 +223,19 @@ PYBIND11_MODULE(_lightspeed, m)
     }, "algorithmic flops since the last reset_stats, by J/K and precision");
     m.def("class_counts", []() {
         // quartets per class: {"fp64"|"fp32": {"J": {(LB,LK): n}, "K": {(L1,L2,L3,L4): n}}}
-        std::vector<unsigned long long> h(2 * (25 + 81));
+        constexpr int NH = 2 * LSJK_LMAX + 1, NL = LSJK_LMAX + 1, NJ = LSJK_NJCLASS, NK = LSJK_NKCLASS;
+        std::vector<unsigned long long> h(2 * (NJ + NK));
         check_rc(lsjk_context_counters(Engine::instance().ctx(), h.data(), (int) h.size()), "class_counts");
         py::dict out;
         for (int prec = 0; prec < 2; ++prec) {
             py::dict j, k;
-            const unsigned long long* b = h.data() + prec * (25 + 81);
-            for (int LB = 0; LB < 5; ++LB)
-                for (int LK = 0; LK < 5; ++LK)
-                    if (b[LB * 5 + LK]) j[py::make_tuple(LB, LK)] = b[LB * 5 + LK];
-            for (int c = 0; c < 81; ++c)
-                if (b[25 + c]) k[py::make_tuple(c / 27, (c / 9) % 3, (c / 3) % 3, c % 3)] = b[25 + c];
+            const unsigned long long* b = h.data() + prec * (NJ + NK);
+            for (int LB = 0; LB < NH; ++LB)
+                for (int LK = 0; LK < NH; ++LK)
+                    if (b[LB * NH + LK]) j[py::make_tuple(LB, LK)] = b[LB * NH + LK];
+            for (int c = 0; c < NK; ++c)
+                if (b[NJ + c])
+                    k[py::make_tuple(c / (NL * NL * NL), (c / (NL * NL)) % NL, (c / NL) % NL, c % NL)] = b[NJ + c];
             py::dict d;
             d["J"] = j;
             d["K"] = k;

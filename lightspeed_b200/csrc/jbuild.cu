@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cub/device/device_radix_sort.cuh>
 #include <optional>
+#include <type_traits>
 #include "engine.cuh"
 #include "hermite.cuh"
 #include "jargs.cuh"
@@ -98,6 +99,22 @@ __global__ void k_bra_count(const unsigned* __restrict__ maxbits, float thresp, 
         if (b[mid] >= thre) lo = mid + 1; else hi = mid;
     }
     nbra[c] = lo;
+}
+
+// The (L1, LB - L1) split of a pair of Hermite class LB whose first shell has
+// angular momentum l1, as a compile-time constant: calls f(integral_constant<L1>)
+// for the one split with L1 == l1 (shells up to kLmax on either side).
+template <int LB, int L1 = (LB > kLmax ? LB - kLmax : 0), typename F>
+__device__ __forceinline__ void with_split(int l1, F&& f)
+{
+    if constexpr (L1 < kLmax && L1 < LB) {
+        if (l1 == L1)
+            f(std::integral_constant<int, L1>{});
+        else
+            with_split<LB, L1 + 1>(l1, f);
+    } else {
+        f(std::integral_constant<int, L1>{});
+    }
 }
 
 // ---- 3. ket Hermite densities -------------------------------------------------
@@ -188,14 +205,10 @@ __global__ void k_ket_herm(const int* __restrict__ perm, const int* __restrict__
     double* r = rec + (long) k * S;
     const double* g = geom + 4L * src;
     // L3 + L4 == LK
-    if (LK == 0) ket_record<0, 0>(i, j, b3, b4, symm, Dc, g, r);
-    else if (LK == 1) { if (L3 == 1) ket_record<1, 0>(i, j, b3, b4, symm, Dc, g, r); else ket_record<0, 1>(i, j, b3, b4, symm, Dc, g, r); }
-    else if (LK == 2) {
-        if (L3 == 2) ket_record<2, 0>(i, j, b3, b4, symm, Dc, g, r);
-        else if (L3 == 1) ket_record<1, 1>(i, j, b3, b4, symm, Dc, g, r);
-        else ket_record<0, 2>(i, j, b3, b4, symm, Dc, g, r);
-    } else if (LK == 3) { if (L3 == 2) ket_record<2, 1>(i, j, b3, b4, symm, Dc, g, r); else ket_record<1, 2>(i, j, b3, b4, symm, Dc, g, r); }
-    else ket_record<2, 2>(i, j, b3, b4, symm, Dc, g, r);
+    with_split<LK>(L3, [&](auto c) {
+        constexpr int A3 = decltype(c)::value;
+        ket_record<A3, LK - A3>(i, j, b3, b4, symm, Dc, g, r);
+    });
     (void) L4;
     if (rec32) {
         float* r32 = rec32 + (long) k * S;
@@ -217,13 +230,14 @@ __global__ void k_ket_bounds(const unsigned* __restrict__ keys_sorted, const int
 
 // Hermite index t -> (tx, ty, tz) as a compile-time table (so unrolled loops
 // index registers, not memory).
+constexpr int kHermTab = nherm_of(2 * kLmax + 1);   // Hermite orders up to the gradients' bra classes
 struct HermTab {
-    int x[56], y[56], z[56];   // Hermite orders up to 5 (the gradients' bra classes)
+    int x[kHermTab], y[kHermTab], z[kHermTab];
 };
 __host__ __device__ constexpr HermTab make_herm_tab()
 {
     HermTab T{};
-    for (int t = 0; t < 56; ++t) {
+    for (int t = 0; t < kHermTab; ++t) {
         T.x[t] = herm_tx(t);
         T.y[t] = herm_ty(t);
         T.z[t] = herm_tz(t);
@@ -232,14 +246,14 @@ __host__ __device__ constexpr HermTab make_herm_tab()
 }
 
 // Cartesian exponents (lx, ly, lz) of component k of a shell of angular
-// momentum L <= 2, as a compile-time table.
+// momentum L <= kLmax, as a compile-time table.
 struct CartTab {
-    int x[3][6], y[3][6], z[3][6];
+    int x[kNL][ncart_of(kLmax)], y[kNL][ncart_of(kLmax)], z[kNL][ncart_of(kLmax)];
 };
 __host__ __device__ constexpr CartTab make_cart_tab()
 {
     CartTab T{};
-    for (int L = 0; L <= 2; ++L)
+    for (int L = 0; L <= kLmax; ++L)
         for (int k = 0; k < ncart_of(L); ++k) {
             T.x[L][k] = cart_lx(L, k);
             T.y[L][k] = cart_ly(L, k);
@@ -302,14 +316,10 @@ __global__ void k_herm_to_cart(const int* __restrict__ nbra, const int* __restri
     int L1 = b1.L[i];
     const double* g = geom + 4L * k;
     const double* jt = jbra + (long) k * H;
-    if (LB == 0) bra_to_cart<0, 0>(i, j, b1, b2, symm, g, jt, Jc);
-    else if (LB == 1) { if (L1 == 1) bra_to_cart<1, 0>(i, j, b1, b2, symm, g, jt, Jc); else bra_to_cart<0, 1>(i, j, b1, b2, symm, g, jt, Jc); }
-    else if (LB == 2) {
-        if (L1 == 2) bra_to_cart<2, 0>(i, j, b1, b2, symm, g, jt, Jc);
-        else if (L1 == 1) bra_to_cart<1, 1>(i, j, b1, b2, symm, g, jt, Jc);
-        else bra_to_cart<0, 2>(i, j, b1, b2, symm, g, jt, Jc);
-    } else if (LB == 3) { if (L1 == 2) bra_to_cart<2, 1>(i, j, b1, b2, symm, g, jt, Jc); else bra_to_cart<1, 2>(i, j, b1, b2, symm, g, jt, Jc); }
-    else bra_to_cart<2, 2>(i, j, b1, b2, symm, g, jt, Jc);
+    with_split<LB>(L1, [&](auto c) {
+        constexpr int A1 = decltype(c)::value;
+        bra_to_cart<A1, LB - A1>(i, j, b1, b2, symm, g, jt, Jc);
+    });
 }
 
 // The same transform for the high bra classes (LB >= 3), a warp per bra
@@ -358,7 +368,7 @@ __global__ void k_herm_to_cart_warp(const int* __restrict__ nbra, const int* __r
 #pragma unroll
         for (int t = 0; t < V; ++t) e.v[t] = t == 0 ? 1.0 : 0.0;
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+        for (int r = 0; r < LB; ++r) {
             if (r >= n1 + n2) break;
             const double X = r < n1 ? XA : XB;
             Ev n;
@@ -397,6 +407,9 @@ void launch_j_row(Context* ctx, const JArgs& A, int LK, int nbra_full, int nket_
     case 2: launch_j<LB, 2>(ctx, A, nbra_full, nket_full); break;
     case 3: launch_j<LB, 3>(ctx, A, nbra_full, nket_full); break;
     case 4: launch_j<LB, 4>(ctx, A, nbra_full, nket_full); break;
+    case 5: launch_j<LB, 5>(ctx, A, nbra_full, nket_full); break;
+    case 6: launch_j<LB, 6>(ctx, A, nbra_full, nket_full); break;
+    default: throw Error(LSJK_ENOTSUPP, "J: ket Hermite class above 6");
     }
 }
 
@@ -485,14 +498,10 @@ __global__ void k_bra_grad(const int* __restrict__ nbra, const int* __restrict__
     int L1 = b1.L[i];
     const double* g = geom + 4L * k;
     const double* vt = vbra + (long) k * H;
-    if (LB == 0) bra_grad<0, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
-    else if (LB == 1) { if (L1 == 1) bra_grad<1, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G); else bra_grad<0, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G); }
-    else if (LB == 2) {
-        if (L1 == 2) bra_grad<2, 0>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
-        else if (L1 == 1) bra_grad<1, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
-        else bra_grad<0, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
-    } else if (LB == 3) { if (L1 == 2) bra_grad<2, 1>(i, j, b1, b2, symm, g, vt, Dc, scale, G); else bra_grad<1, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G); }
-    else bra_grad<2, 2>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+    with_split<LB>(L1, [&](auto c) {
+        constexpr int A1 = decltype(c)::value;
+        bra_grad<A1, LB - A1>(i, j, b1, b2, symm, g, vt, Dc, scale, G);
+    });
 }
 
 // Algorithmic FP64/FP32 flops of one J quartet of Hermite class (LB|LK):
@@ -564,6 +573,9 @@ KetSet prepare_kets(Context* ctx, const PairList* pl12, const PairList* pl34, co
         case 2: k_ket_herm<2><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
         case 3: k_ket_herm<3><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
         case 4: k_ket_herm<4><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 5: k_ket_herm<5><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        case 6: k_ket_herm<6><<<nblk(n, 128), 128, 0, s>>>(perm, nk, jk.p1.p, jk.p2.p, jk.bound.p, jk.geom.p, b3->view(), b4->view(), pl34->symm, DS, krec, krec32); break;
+        default: throw Error(LSJK_ENOTSUPP, "J: ket Hermite class above 6");
         }
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches += 7;
@@ -664,6 +676,9 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
                 case 2: launch_j_row<2>(ctx, X, LK, jb.n, jk.n); break;
                 case 3: launch_j_row<3>(ctx, X, LK, jb.n, jk.n); break;
                 case 4: launch_j_row<4>(ctx, X, LK, jb.n, jk.n); break;
+                case 5: launch_j_row<5>(ctx, X, LK, jb.n, jk.n); break;
+                case 6: launch_j_row<6>(ctx, X, LK, jb.n, jk.n); break;
+                default: throw Error(LSJK_ENOTSUPP, "J: bra Hermite class above 6");
                 }
             };
             if (ctx->tuning) {
@@ -713,6 +728,9 @@ void coulomb_build(Context* ctx, const Ewald& ew, const PairList* pl12, const Pa
             case 2: k_herm_to_cart<2><<<gr, 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
             case 3: k_herm_to_cart_warp<3><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
             case 4: k_herm_to_cart_warp<4><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 5: k_herm_to_cart_warp<5><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            case 6: k_herm_to_cart_warp<6><<<nblk(jb.n, 4), 128, 0, s>>>(nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, b1->view(), b2->view(), pl12->symm, jt, Jc); break;
+            default: throw Error(LSJK_ENOTSUPP, "J: bra Hermite class above 6");
             }
             LSJK_CUDA(cudaGetLastError());
             ctx->stats.kernel_launches++;
@@ -773,6 +791,9 @@ static void coulomb_grad_bra(Context* ctx, const Ewald& ew, const PairList* pl, 
             case 3: launch_j_row<3>(ctx, A, LK, jb.n, jk.n); break;
             case 4: launch_j_row<4>(ctx, A, LK, jb.n, jk.n); break;
             case 5: launch_j_row<5>(ctx, A, LK, jb.n, jk.n); break;
+            case 6: launch_j_row<6>(ctx, A, LK, jb.n, jk.n); break;
+            case 7: launch_j_row<7>(ctx, A, LK, jb.n, jk.n); break;
+            default: throw Error(LSJK_ENOTSUPP, "J gradient: bra Hermite class above 7");
             }
         }
         const BasisView v1 = pl->b1->view(), v2 = pl->b2->view();
@@ -783,6 +804,9 @@ static void coulomb_grad_bra(Context* ctx, const Ewald& ew, const PairList* pl, 
         case 2: k_bra_grad<2><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
         case 3: k_bra_grad<3><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
         case 4: k_bra_grad<4><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 5: k_bra_grad<5><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        case 6: k_bra_grad<6><<<gr, 64, 0, s>>>(KS.nbra + LB, jb.p1.p, jb.p2.p, jb.geom.p, v1, v2, pl->symm, vbra, Dbra, scale, G); break;
+        default: throw Error(LSJK_ENOTSUPP, "J gradient: bra Hermite class above 6");
         }
         LSJK_CUDA(cudaGetLastError());
         ctx->stats.kernel_launches++;

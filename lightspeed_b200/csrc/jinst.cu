@@ -1,5 +1,5 @@
 // Instantiates the J kernels of one bra Hermite class (compiled once per
-// LSJK_LB = 0..4 by the build).
+// LSJK_LB = 0..2 kLmax + 1 by the build) against every ket Hermite class.
 #include "jkernel.cuh"
 
 #ifndef LSJK_LB
@@ -12,4 +12,6 @@ template void launch_j<LSJK_LB, 1>(Context*, const JArgs&, int, int);
 template void launch_j<LSJK_LB, 2>(Context*, const JArgs&, int, int);
 template void launch_j<LSJK_LB, 3>(Context*, const JArgs&, int, int);
 template void launch_j<LSJK_LB, 4>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 5>(Context*, const JArgs&, int, int);
+template void launch_j<LSJK_LB, 6>(Context*, const JArgs&, int, int);
 } // namespace lsjk

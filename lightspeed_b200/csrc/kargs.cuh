@@ -128,7 +128,10 @@ struct KGradArgs {
     double alpha[4], omega[4];
 };
 
-// One (L1 L2|L3 L4) class of the K gradient (cap: the class's task capacity).
+// One (L1 L2|L3 L4) class of the K gradient (cap: the class's task capacity);
+// launch_k_grad_l1<L1> holds the classes of one partner-1 shell.
 void launch_k_grad(Context* ctx, const KGradArgs& A, long cap, int L1, int L2, int L3, int L4);
+template <int L1>
+void launch_k_grad_l1(Context* ctx, const KGradArgs& A, long cap, int L2, int L3, int L4);
 
 } // namespace lsjk

@@ -189,6 +189,8 @@ void launch_k4(Context* ctx, const KArgs& A, long cap, int L4, bool fp32)
     case 0: launch_k<L1, L2, L3, 0>(ctx, A, cap, fp32); break;
     case 1: launch_k<L1, L2, L3, 1>(ctx, A, cap, fp32); break;
     case 2: launch_k<L1, L2, L3, 2>(ctx, A, cap, fp32); break;
+    case 3: launch_k<L1, L2, L3, 3>(ctx, A, cap, fp32); break;
+    default: throw Error(LSJK_ENOTSUPP, "K: shell above f");
     }
 }
 template <int L1, int L2>
@@ -198,6 +200,8 @@ void launch_k3(Context* ctx, const KArgs& A, long cap, int L3, int L4, bool fp32
     case 0: launch_k4<L1, L2, 0>(ctx, A, cap, L4, fp32); break;
     case 1: launch_k4<L1, L2, 1>(ctx, A, cap, L4, fp32); break;
     case 2: launch_k4<L1, L2, 2>(ctx, A, cap, L4, fp32); break;
+    case 3: launch_k4<L1, L2, 3>(ctx, A, cap, L4, fp32); break;
+    default: throw Error(LSJK_ENOTSUPP, "K: shell above f");
     }
 }
 template <int L1>
@@ -207,6 +211,8 @@ void launch_k2(Context* ctx, const KArgs& A, long cap, int L2, int L3, int L4, b
     case 0: launch_k3<L1, 0>(ctx, A, cap, L3, L4, fp32); break;
     case 1: launch_k3<L1, 1>(ctx, A, cap, L3, L4, fp32); break;
     case 2: launch_k3<L1, 2>(ctx, A, cap, L3, L4, fp32); break;
+    case 3: launch_k3<L1, 3>(ctx, A, cap, L3, L4, fp32); break;
+    default: throw Error(LSJK_ENOTSUPP, "K: shell above f");
     }
 }
 void launch_k1(Context* ctx, const KArgs& A, long cap, int L1, int L2, int L3, int L4, bool fp32)
@@ -215,6 +221,8 @@ void launch_k1(Context* ctx, const KArgs& A, long cap, int L1, int L2, int L3, i
     case 0: launch_k2<0>(ctx, A, cap, L2, L3, L4, fp32); break;
     case 1: launch_k2<1>(ctx, A, cap, L2, L3, L4, fp32); break;
     case 2: launch_k2<2>(ctx, A, cap, L2, L3, L4, fp32); break;
+    case 3: launch_k2<3>(ctx, A, cap, L2, L3, L4, fp32); break;
+    default: throw Error(LSJK_ENOTSUPP, "K: shell above f");
     }
 }
 
@@ -255,9 +263,12 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
 
-    // per-combo task regions: capacity = prims of L2 in basis2 x prims of L4 in basis4
-    int cnt2[kNL] = {0}, cnt4[kNL] = {0};
+    // per-combo task regions: capacity = prims of L2 in basis2 x prims of L4 in basis4,
+    // none where basis 1 has no partner of L1 or basis 3 none of L3 (no task can name it)
+    int cnt1[kNL] = {0}, cnt2[kNL] = {0}, cnt3[kNL] = {0}, cnt4[kNL] = {0};
+    for (int L : pl12->b1->L) cnt1[L]++;
     for (int L : b2->L) cnt2[L]++;
+    for (int L : pl34->b1->L) cnt3[L]++;
     for (int L : b4->L) cnt4[L]++;
     std::vector<long> off(kNCombo + 1, 0);
     for (int L1 = 0; L1 < kNL; ++L1)
@@ -265,7 +276,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
             for (int L3 = 0; L3 < kNL; ++L3)
                 for (int L4 = 0; L4 < kNL; ++L4) {
                     int c = combo_index(L1, L2, L3, L4);
-                    off[c + 1] = (long) cnt2[L2] * cnt4[L4] * ngroup;
+                    off[c + 1] = (cnt1[L1] && cnt3[L3]) ? (long) cnt2[L2] * cnt4[L4] * ngroup : 0L;
                 }
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     const bool mixed = ctx->precision == LSJK_PREC_MIXED && thredp > thresp;
@@ -491,7 +502,8 @@ void exchange_grad(Context* ctx, const Ewald& ew, const PairList* pl, const doub
     for (int L1 = 0; L1 < kNL; ++L1)
         for (int L2 = 0; L2 < kNL; ++L2)
             for (int L3 = 0; L3 < kNL; ++L3)
-                for (int L4 = 0; L4 < kNL; ++L4) off[combo_index(L1, L2, L3, L4) + 1] = (long) cnt[L2] * cnt[L4];
+                for (int L4 = 0; L4 < kNL; ++L4)
+                    off[combo_index(L1, L2, L3, L4) + 1] = (cnt[L1] && cnt[L3]) ? (long) cnt[L2] * cnt[L4] : 0L;
     for (int c = 0; c < kNCombo; ++c) off[c + 1] += off[c];
     KTask* tasks = take<KTask>(ctx, off[kNCombo]);
     int* ntask = take<int>(ctx, kNCombo);

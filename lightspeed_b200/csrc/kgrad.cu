@@ -17,10 +17,15 @@
 // small local arrays: this is not the hot path. Contributions collect per atom
 // in registers (partner-1 atom: warp-uniform; prim2 and prim4: per task;
 // partner-3: per lane) and reach G with few atomics.
+#include <atomic>
 #include "engine.cuh"
 #include "kargs.cuh"
 #include "lsjk_device.cuh"
 #include "hermite.cuh"   // cart_lx/ly/lz
+
+#ifndef LSJK_KG_L1
+#error "compile with -DLSJK_KG_L1=<partner-1 shell>"
+#endif
 
 namespace lsjk {
 
@@ -484,7 +489,9 @@ template <int L1, int L2, int L3, int L4>
 __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constant__ KGradArgs A)
 {
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
-    __shared__ KGradWarpTables<L1, L2, L3, L4> tabs[4];
+    // four warps' tables (dynamic: the f classes need more than 48 KB)
+    extern __shared__ __align__(16) unsigned char kgrad_smem[];
+    auto* tabs = reinterpret_cast<KGradWarpTables<L1, L2, L3, L4>*>(kgrad_smem);
     KGradWarpTables<L1, L2, L3, L4>& S = tabs[threadIdx.x >> 5];
     const int ntask = *A.ntask;
     const int lane = threadIdx.x & 31;
@@ -568,9 +575,20 @@ template <int L1, int L2, int L3, int L4>
 void launch_one(Context* ctx, const KGradArgs& A, long cap)
 {
     const unsigned grid = (unsigned) std::min<long>((cap + 3) / 4, (long) ctx->nsm * 8);
-    if constexpr (kgrad_warp<L1, L2, L3, L4>())
-        k_exchange_grad_warp<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
-    else
+    if constexpr (kgrad_warp<L1, L2, L3, L4>()) {
+        constexpr size_t smem = 4 * sizeof(KGradWarpTables<L1, L2, L3, L4>);
+        auto kern = k_exchange_grad_warp<L1, L2, L3, L4>;
+        if constexpr (smem > 48 * 1024) {
+            // the opt-in is a per-device function attribute: set it once per device
+            static std::atomic<unsigned long long> devices{0};
+            const unsigned long long bit = 1ull << (ctx->device & 63);
+            if (!(devices.load(std::memory_order_acquire) & bit)) {
+                LSJK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+                devices.fetch_or(bit, std::memory_order_acq_rel);
+            }
+        }
+        kern<<<grid, 128, smem, ctx->stream>>>(A);
+    } else
         k_exchange_grad<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
@@ -583,6 +601,8 @@ void launch4(Context* ctx, const KGradArgs& A, long cap, int L4)
     case 0: launch_one<L1, L2, L3, 0>(ctx, A, cap); break;
     case 1: launch_one<L1, L2, L3, 1>(ctx, A, cap); break;
     case 2: launch_one<L1, L2, L3, 2>(ctx, A, cap); break;
+    case 3: launch_one<L1, L2, L3, 3>(ctx, A, cap); break;
+    default: throw Error(LSJK_ENOTSUPP, "K gradient: shell above f");
     }
 }
 template <int L1, int L2>
@@ -592,6 +612,8 @@ void launch3(Context* ctx, const KGradArgs& A, long cap, int L3, int L4)
     case 0: launch4<L1, L2, 0>(ctx, A, cap, L4); break;
     case 1: launch4<L1, L2, 1>(ctx, A, cap, L4); break;
     case 2: launch4<L1, L2, 2>(ctx, A, cap, L4); break;
+    case 3: launch4<L1, L2, 3>(ctx, A, cap, L4); break;
+    default: throw Error(LSJK_ENOTSUPP, "K gradient: shell above f");
     }
 }
 template <int L1>
@@ -601,19 +623,34 @@ void launch2(Context* ctx, const KGradArgs& A, long cap, int L2, int L3, int L4)
     case 0: launch3<L1, 0>(ctx, A, cap, L3, L4); break;
     case 1: launch3<L1, 1>(ctx, A, cap, L3, L4); break;
     case 2: launch3<L1, 2>(ctx, A, cap, L3, L4); break;
+    case 3: launch3<L1, 3>(ctx, A, cap, L3, L4); break;
+    default: throw Error(LSJK_ENOTSUPP, "K gradient: shell above f");
     }
 }
 
 } // namespace
 
+// This unit holds the classes with partner-1 shell LSJK_KG_L1 (the build compiles
+// it once per shell, so the classes compile in parallel).
+template <int L1>
+void launch_k_grad_l1(Context* ctx, const KGradArgs& A, long cap, int L2, int L3, int L4)
+{
+    launch2<L1>(ctx, A, cap, L2, L3, L4);
+}
+template void launch_k_grad_l1<LSJK_KG_L1>(Context*, const KGradArgs&, long, int, int, int);
+
+#if LSJK_KG_L1 == 0
 void launch_k_grad(Context* ctx, const KGradArgs& A, long cap, int L1, int L2, int L3, int L4)
 {
     if (cap == 0) return;
     switch (L1) {
-    case 0: launch2<0>(ctx, A, cap, L2, L3, L4); break;
-    case 1: launch2<1>(ctx, A, cap, L2, L3, L4); break;
-    case 2: launch2<2>(ctx, A, cap, L2, L3, L4); break;
+    case 0: launch_k_grad_l1<0>(ctx, A, cap, L2, L3, L4); break;
+    case 1: launch_k_grad_l1<1>(ctx, A, cap, L2, L3, L4); break;
+    case 2: launch_k_grad_l1<2>(ctx, A, cap, L2, L3, L4); break;
+    case 3: launch_k_grad_l1<3>(ctx, A, cap, L2, L3, L4); break;
+    default: throw Error(LSJK_ENOTSUPP, "K gradient: shell above f");
     }
 }
+#endif
 
 } // namespace lsjk

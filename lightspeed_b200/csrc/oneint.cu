@@ -198,8 +198,10 @@ void launch_one(Context* ctx, const OneArgs& A, int LA, int LB)
     if (LA == a && LB == b) {                                              \
         k_oneint<a, b, KIND><<<grid, 128, 0, s>>>(A);                      \
     }
-    LSJK_ONE(0, 0) LSJK_ONE(0, 1) LSJK_ONE(0, 2) LSJK_ONE(1, 0) LSJK_ONE(1, 1) LSJK_ONE(1, 2)
-    LSJK_ONE(2, 0) LSJK_ONE(2, 1) LSJK_ONE(2, 2)
+#define LSJK_ONE_ROW(a) LSJK_ONE(a, 0) else LSJK_ONE(a, 1) else LSJK_ONE(a, 2) else LSJK_ONE(a, 3)
+    LSJK_ONE_ROW(0) else LSJK_ONE_ROW(1) else LSJK_ONE_ROW(2) else LSJK_ONE_ROW(3) else
+        throw Error(LSJK_ENOTSUPP, "one-electron integrals: shell above f");
+#undef LSJK_ONE_ROW
 #undef LSJK_ONE
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;

@@ -1,0 +1,134 @@
+"""f shells: classes with an f shell run the loop form of the quartet code
+(quartet_loops.cuh) inside the same J/K kernels, one-electron kernels and
+gradients as the lighter classes. Checked against the oracle (the reference CPU
+IntBox, which takes any angular momentum) on a water dimer in cc-pVTZ
+(spherical f on oxygen, d on hydrogen) and in a Cartesian copy of it:
+
+* pair list identical, J, symmetric and non-symmetric K elementwise 1e-10
+  (FP64), 1e-6 in mixed precision at thredp 1e-6;
+* range-separated J and K (erf-attenuated and a two-term operator) at 1e-10;
+* S, T at 1e-12 and V at 1e-10;
+* the J and K gradients at 1e-9 (K: the fully symmetric routine, the mirror
+  halving of two symmetric densities, and the unpromised path)."""
+import numpy as np
+import pytest
+
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _dimer(ls, spherical=None):
+    from lightspeed_b200.geometry import water_cluster
+    mol = water_cluster(2, seed=1)
+    bas = ls.Basis.from_gbs_file(mol, "cc-pvtz", spherical=spherical)
+    return mol, bas
+
+
+def _densities(bas, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((bas.nao, 10)) / np.sqrt(bas.nao)
+    Y = rng.standard_normal((bas.nao, 10)) / np.sqrt(bas.nao)
+    D = X @ X.T
+    Dn = D + 0.05 * (X @ Y.T)
+    return D, Dn
+
+
+@pytest.fixture(scope="module")
+def oracle_ok():
+    if not ref.available():
+        pytest.skip("oracle/_ref not built")
+
+
+@pytest.mark.parametrize("spherical", [None, False])
+def test_fshell_jk_vs_oracle(ls, oracle_ok, spherical):
+    mol, bas = _dimer(ls, spherical)
+    assert max(p.L for p in bas.primitives) == 3
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    got = [(l.L1, l.L2, p.prim1.primIdx, p.prim2.primIdx, p.bound) for l in pl.pairlists for p in l.pairs]
+    L1, L2, p1, p2, b = rp.export()
+    assert np.array_equal(np.array([x[:4] for x in got]), np.stack([L1, L2, p1, p2], 1))
+    gb = np.array([x[4] for x in got], np.float32)
+    assert np.all(np.abs(gb.view(np.int32) - b.view(np.int32)) <= 1)
+    D, Dn = _densities(bas, 7)
+    J = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), 1e-14, 1e-14).np
+    Jr = ref.coulomb(rp, rp, D, 1e-14, 1e-14)
+    assert np.max(np.abs(Jr)) > 1.0
+    assert np.max(np.abs(J - Jr)) < 1e-10
+    K = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-14).np
+    assert np.max(np.abs(K - ref.exchange(rp, rp, D, True, 1e-14, 1e-14))) < 1e-10
+    Kn = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(Dn), False, 1e-14, 1e-14).np
+    assert np.max(np.abs(Kn - ref.exchange(rp, rp, Dn, False, 1e-14, 1e-14))) < 1e-10
+    # mixed precision: FP32 below thredp, FP64 accumulation
+    Jm = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), 1e-14, 1e-6).np
+    Km = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-6).np
+    assert np.max(np.abs(Jm - Jr)) < 1e-6
+    assert np.max(np.abs(Km - K)) < 1e-6
+
+
+def test_fshell_range_separated(ls, oracle_ok):
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    D, _ = _densities(bas, 8)
+    for sc, om in (([1.0], [0.4]), ([0.6, 0.4], [-1.0, 0.3])):
+        ew = ls.Ewald(sc, om)
+        J = ls.IntBox.coulomb(res, ew, pl, pl, ls.Tensor.array(D), 1e-14, 1e-14).np
+        assert np.max(np.abs(J - ref.coulomb(rp, rp, D, 1e-14, 1e-14, sc, om))) < 1e-10
+        K = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-14).np
+        assert np.max(np.abs(K - ref.exchange(rp, rp, D, True, 1e-14, 1e-14, sc, om))) < 1e-10
+
+
+def test_fshell_one_electron(ls, oracle_ok):
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    assert np.max(np.abs(ls.IntBox.overlap(res, pl).np - ref.overlap(rp))) < 1e-12
+    assert np.max(np.abs(ls.IntBox.kinetic(res, pl).np - ref.kinetic(rp))) < 1e-12
+    V = ls.IntBox.potential(res, ls.Ewald.coulomb(), pl, ls.Tensor.array(mol.xyzZ)).np
+    assert np.max(np.abs(V - ref.potential(rp, mol.xyzZ))) < 1e-10
+
+
+def test_fshell_coulomb_grad(ls, oracle_ok):
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    D, _ = _densities(bas, 9)
+    _, Db = _densities(bas, 10)
+    Db = 0.5 * (Db + Db.T)
+    A, B = ls.Tensor.array(D), ls.Tensor.array(Db)
+    G = ls.IntBox.coulombGrad(res, ls.Ewald.coulomb(), pl, A, B, 1e-14, 1e-14).np
+    Gr = ref.coulomb_grad(rp, D, Db, 1e-14, 1e-14)
+    assert np.max(np.abs(Gr)) > 1e-3
+    assert np.max(np.abs(G - Gr)) < 1e-9
+
+
+def test_fshell_exchange_grad(ls, oracle_ok):
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    Da, _ = _densities(bas, 11)
+    Db, _ = _densities(bas, 12)
+    A, B = ls.Tensor.array(Da), ls.Tensor.array(Db)
+    G_same = ls.IntBox.exchangeGrad(res, ew, pl, A, A, True, True, True, 1e-14, 1e-14).np
+    Gr_same = ref.exchange_grad(rp, Da, None, True, True, 1e-14, 1e-14)
+    assert np.max(np.abs(Gr_same)) > 1e-3
+    assert np.max(np.abs(G_same - Gr_same)) < 1e-9
+    G_ab = ls.IntBox.exchangeGrad(res, ew, pl, A, B, True, True, False, 1e-14, 1e-14).np
+    Gr_ab = ref.exchange_grad(rp, Da, Db, True, True, 1e-14, 1e-14)
+    assert np.max(np.abs(G_ab - Gr_ab)) < 1e-9
+    G_nosym = ls.IntBox.exchangeGrad(res, ew, pl, A, B, False, False, False, 1e-14, 1e-14).np
+    assert np.max(np.abs(G_nosym - Gr_ab)) < 1e-9
