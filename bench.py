@@ -46,12 +46,13 @@ def parse():
                     help="alkane: K over the primitives as given (the reference's exact quartet set) instead of "
                          "the merged twins")
     ap.add_argument("--scf-maxiter", type=int, default=60)
-    ap.add_argument("--workload", default="alkane", choices=["alkane", "batched", "guess", "many", "eri", "grad"],
+    ap.add_argument("--workload", default="alkane",
+                    choices=["alkane", "batched", "guess", "many", "eri", "grad", "fshell"],
                     help="alkane: the headline C40H82 J+K step; batched: 64 response-like densities "
                          "of a 32-water cluster per step (one line per operator and precision); guess: "
                          "train the learned SCF guess and time SCFs from it against SAD")
     ap.add_argument("--molecules", type=int, default=512, help="many: number of water clusters")
-    ap.add_argument("--waters", type=int, default=16, help="eri: water cluster size")
+    ap.add_argument("--waters", type=int, default=16, help="eri: water cluster size (fshell: 4 unless given)")
     ap.add_argument("--active", type=int, default=12, help="eri: active orbitals")
     ap.add_argument("--train-clusters", type=int, default=1000)
     ap.add_argument("--test-clusters", type=int, default=20)
@@ -759,6 +760,92 @@ def run_grad(args):
     return 0
 
 
+def run_fshell(args):
+    """Classes with f shells: a water cluster (`--waters`, default here 4, seed 0)
+    in cc-pVTZ (spherical f on O, d on H), Schwarz and thresp 1e-12, a symmetric
+    density of rank 5 per water (seeded normal columns). A step is one J+K build
+    through the host API (D in, J and K out, host arrays) timed on the wall clock
+    around the synchronous calls, in FP64 and in mixed precision (thredp 1e-6);
+    the J+K nuclear gradients (FP64, the fully symmetric calls) are timed the same
+    way. `value` = FP64 J+K builds per second. The reference's CPU routines
+    (oracle/_ref, all host cores) run once on the same inputs, and the results are
+    compared elementwise."""
+    rank, world, local = dist_info()
+    import torch
+    torch.cuda.set_device(local)
+    import lightspeed_b200 as ls
+    from lightspeed_b200.geometry import water_cluster
+    from oracle import ref
+    if rank != 0:
+        return 0
+    nw = args.waters if args.waters != 16 else 4
+    mol = water_cluster(nw, seed=0)
+    bas = ls.Basis.from_gbs_file(mol, "cc-pvtz")
+    thre = 1.0e-12
+    res = ls.ResourceList.build()
+    pl = ls.PairList.build_schwarz(bas, bas, True, thre)
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((bas.nao, 5 * nw)) / np.sqrt(bas.nao)
+    D = X @ X.T
+    Dt = ls.Tensor.array(D)
+    ew = ls.Ewald.coulomb()
+
+    def build(thredp):
+        J = ls.IntBox.coulomb(res, ew, pl, pl, Dt, thre, thredp)
+        K = ls.IntBox.exchange(res, ew, pl, pl, Dt, True, thre, thredp)
+        return J.np.copy(), K.np.copy()
+
+    def grads():
+        GJ = ls.IntBox.coulombGrad(res, ew, pl, Dt, Dt, thre, thre)
+        GK = ls.IntBox.exchangeGrad(res, ew, pl, Dt, Dt, True, True, True, thre, thre)
+        return GJ.np.copy(), GK.np.copy()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            out = fn()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            out = fn()
+            ts.append(time.perf_counter() - t0)
+        return out, 1e3 * float(np.mean(ts))
+
+    ls.set_precision(ls.PREC_FP64)
+    (J, K), ms64 = timed(lambda: build(thre))
+    ls.set_precision(ls.PREC_MIXED)
+    (Jm, Km), msmx = timed(lambda: build(1e-6))
+    ls.set_precision(ls.PREC_FP64)
+    (GJ, GK), msg = timed(grads)
+    cpu = None
+    if ref.available() and not args.no_cpu_baseline:
+        rb = ref.RefBasis(ref.prim_arrays(bas))
+        rp = ref.RefPairs(rb, rb, True, thre)
+        nthread = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        RJ = ref.coulomb(rp, rp, D, thre, thre, nthread=nthread)
+        RK = ref.exchange(rp, rp, D, True, thre, thre, nthread=nthread)
+        t1 = time.perf_counter()
+        RGJ = ref.coulomb_grad(rp, D, None, thre, thre, nthread=nthread)
+        RGK = ref.exchange_grad(rp, D, None, True, True, thre, thre, nthread=nthread)
+        t2 = time.perf_counter()
+        cpu = {"kind": "reference", "cores": nthread, "cpu_model": cpu_model(), "ms_jk": 1e3 * (t1 - t0),
+               "ms_grad": 1e3 * (t2 - t1), "max_abs_dJ": float(np.max(np.abs(J - RJ))),
+               "max_abs_dK": float(np.max(np.abs(K - RK))), "max_abs_dJ_mixed": float(np.max(np.abs(Jm - RJ))),
+               "max_abs_dK_mixed": float(np.max(np.abs(Km - RK))), "max_abs_dGJ": float(np.max(np.abs(GJ - RGJ))),
+               "max_abs_dGK": float(np.max(np.abs(GK - RGK)))}
+    line = {
+        "metric": "J+K build with f shells: ms per build (FP64, mixed) and builds/s; J+K gradient ms",
+        "value": 1e3 / ms64, "unit": "builds/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms64, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "%d H2O (seed 0) / cc-pVTZ J+K build and gradient" % nw, "nao": bas.nao,
+                   "ncart": bas.ncart, "thresp": thre, "api": "host (D in, J/K or G out)"},
+        "ms_mixed": msmx, "ms_grad": msg, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_eri(args):
     """MO-basis integrals through J builds (IntBox.eriJ, the CASCI integrals):
     a `--waters` H2O cluster (seed 0) in 6-31G*, Schwarz 1e-12, one block of
@@ -1029,6 +1116,8 @@ def main():
         return run_eri(args)
     if args.workload == "grad":
         return run_grad(args)
+    if args.workload == "fshell":
+        return run_fshell(args)
     return run_ours(args)
 
 

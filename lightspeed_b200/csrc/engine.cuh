@@ -28,6 +28,7 @@ namespace lsjk {
 constexpr int kLmax = LSJK_LMAX;               // s, p, d, f shells
 constexpr int kNL = kLmax + 1;
 constexpr int kNHerm = 2 * kLmax + 1;          // Hermite classes L1+L2 = 0..6
+constexpr int kGenLmax = 2;                    // largest shell of the straight-line quartet code
 
 inline int ncart_count(int L) { return (L + 1) * (L + 2) / 2; }
 

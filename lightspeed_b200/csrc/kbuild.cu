@@ -388,14 +388,17 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         A.omega[t] = ew.omega[t];
                     }
                     const float inf = __builtin_huge_valf();
+                    // classes above the straight-line quartet code (an f shell) run in FP64 only:
+                    // one pass over all tasks (their FP32 loop form is no faster than FP64)
+                    const bool two_pass = mixed && std::max(std::max(L1, L2), std::max(L3, L4)) <= kGenLmax;
                     // FP64 pass: estimate >= thredp (mixed) or >= thresp (FP64 mode)
                     A.queue = queue + c;
-                    if (mixed) {
+                    if (two_pass) {
                         // FP64 pass: only the tasks that can reach thredp
                         A.tasks = tasks_hi + off[c];
                         A.ntask = ntask + kNCombo + c;
                     }
-                    A.thr_lo = mixed ? thredp : thresp;
+                    A.thr_lo = two_pass ? thredp : thresp;
                     A.thr_hi = inf;
                     A.rys = ctx->rys64.p + kRysOffset[NR];
                     A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
@@ -440,7 +443,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         if (par) on.emplace(ctx, lane++);
                         launch_k1(ctx, A, cap, L1, L2, L3, L4, false);
                     }
-                    if (mixed) {
+                    if (two_pass) {
                         // FP32 pass: thresp <= estimate < thredp, over all tasks
                         A.tasks = tasks + off[c];
                         A.ntask = ntask + c;

@@ -511,6 +511,12 @@ __global__ void __launch_bounds__(kKThreads) k_exchange(const __grid_constant__ 
     if (lane == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
 }
 
+} // namespace lsjk
+
+#include "kwarp.cuh"
+
+namespace lsjk {
+
 template <int L1, int L2, int L3, int L4, typename R, int NG, bool GC>
 void launch_k_one(Context* ctx, const KArgs& A, unsigned grid)
 {
@@ -575,6 +581,14 @@ void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
             launch_k_gc<L1, L2, L3, L4, float, 1>(ctx, B, grid_for(B.nsub));
         }
     } else {
+        if constexpr (k_warp_class<L1, L2, L3, L4>()) {
+            // heavy f classes: a quartet per warp (partners with one output target)
+            if (!A.gc) {
+                B.nsub = per_group;
+                launch_k_warp<L1, L2, L3, L4>(ctx, B, grid_for(B.nsub));
+                return;
+            }
+        }
         constexpr int NGd = k_batch<L1, L2, L3, L4, double>();
         if (NGd > 1 && per_group >= NGd) {
             B.nsub = (per_group + NGd - 1) / NGd;
