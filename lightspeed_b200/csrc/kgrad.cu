@@ -62,12 +62,14 @@ __host__ __device__ constexpr bool kgrad_flat()
 }
 
 // The heaviest classes (at least 324 Cartesian combinations: (dd|pp), (dp|dp)
-// and above) run one quartet per warp with the tables in shared memory; the
-// rest one quartet per lane.
+// and above; with an f shell, at least 100) run one quartet per warp with the
+// tables in shared memory; the rest one quartet per lane.
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool kgrad_warp()
 {
-    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin;
+    constexpr int nc = ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4);
+    // with an f shell from 100 combinations on: a lane's tables would no longer fit L1
+    return nc >= kGradWarpMin || ((L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) && nc >= 100);
 }
 
 // One quartet's derivatives at centres 1, 2 and 3 contracted with the D13 and
@@ -342,6 +344,10 @@ struct KGradWarpTables {
     double Hb[3][XB][XA][MC + 1];     // after the transfer to centre 2
     double D13[ncart_of(L1) * ncart_of(L3)];
     double D24[ncart_of(L2) * ncart_of(L4)];
+    // per (a <= L1, b <= L2, c <= L3, e <= L4) and direction: the 1-D integral and its
+    // derivatives at centres 1, 2 and 3 (2 alpha X(a+1) - a X(a-1), likewise in b, c)
+    static constexpr int SG = (L1 + 1) * (L2 + 1) * (L3 + 1) * (L4 + 1);
+    double T4[3][SG][4];
 };
 
 // One quartet of a heavy class, computed by the whole warp: lanes 0-2 run the
@@ -359,7 +365,10 @@ __device__ void kgrad_quartet_warp(const KGradArgs& A, KGradWarpTables<L1, L2, L
     constexpr int NR = (L1 + L2 + L3 + L4 + 1) / 2 + 1;
     constexpr int MA = Tab::MA, MC = Tab::MC, XA = Tab::XA, XB = Tab::XB, XC = Tab::XC, XE = Tab::XE;
     constexpr int N1 = ncart_of(L1), N2 = ncart_of(L2), N3 = ncart_of(L3), N4 = ncart_of(L4);
-    constexpr int NC = N1 * N3 * N2 * N4;
+    // contraction jobs: element (i1, i3) of D13, split over P ranges of i2 when there are
+    // fewer elements than lanes
+    constexpr int NO = N1 * N3, NPART = NO >= 32 ? 1 : (N2 < 32 / NO ? N2 : 32 / NO);
+    constexpr int NJOB = NO * NPART, NJL = (NJOB + 31) / 32;
     double PQ[3], PA[3];
     double RR = 0.0;
 #pragma unroll
@@ -444,38 +453,63 @@ __device__ void kgrad_quartet_warp(const KGradArgs& A, KGradWarpTables<L1, L2, L
                 }
             }
             __syncwarp();
-            // the Cartesian combinations (i1, i3, i2, i4) over the lanes
-            for (int cmb = lane; cmb < NC; cmb += 32) {
-                const int i4 = cmb % N4, i2 = (cmb / N4) % N2, i13 = cmb / (N4 * N2);
-                const int i1 = i13 / N3, i3 = i13 % N3;
-                const double W = S.D13[i1 * N3 + i3] * S.D24[i2 * N4 + i4];
-                if (W == 0.0) continue;
-                const int a[3] = {cart_lx(L1, i1), cart_ly(L1, i1), cart_lz(L1, i1)};
-                const int b[3] = {cart_lx(L2, i2), cart_ly(L2, i2), cart_lz(L2, i2)};
-                const int c[3] = {cart_lx(L3, i3), cart_ly(L3, i3), cart_lz(L3, i3)};
-                const int e[3] = {cart_lx(L4, i4), cart_ly(L4, i4), cart_lz(L4, i4)};
-                double v[3], da[3], db[3], dc[3];
+            // the integrals and their derivatives at the (a, b, c, e) of the contraction
+            constexpr int SG = Tab::SG, S2 = L2 + 1, S3 = L3 + 1, S4 = L4 + 1;
+            for (int idx = lane; idx < 3 * SG; idx += 32) {
+                const int d = idx / SG, rr = idx - d * SG;
+                const int e = rr % S4, c = (rr / S4) % S3, b = (rr / (S4 * S3)) % S2, a = rr / (S4 * S3 * S2);
+                double da = 2.0 * alpha * S.X[d][a + 1][b][c][e];
+                if (a) da -= a * S.X[d][a - 1][b][c][e];
+                double db = 2.0 * beta * S.X[d][a][b + 1][c][e];
+                if (b) db -= b * S.X[d][a][b - 1][c][e];
+                double dc = 2.0 * gamma * S.X[d][a][b][c + 1][e];
+                if (c) dc -= c * S.X[d][a][b][c - 1][e];
+                double* o = S.T4[d][rr];
+                o[0] = S.X[d][a][b][c][e];
+                o[1] = da;
+                o[2] = db;
+                o[3] = dc;
+            }
+            __syncwarp();
+            // the contraction: jobs (i1, i3, a range of i2) over the lanes, i4 innermost
+#pragma unroll 1
+            for (int k = 0; k < NJL; ++k) {
+                const int job = lane + 32 * k;
+                if (job >= NJOB) break;
+                const int o13 = job / NPART, part = job % NPART;
+                const double d13 = S.D13[o13];
+                if (d13 == 0.0) continue;
+                const int i1 = o13 / N3, i3 = o13 - (o13 / N3) * N3;
+                const int x1 = cart_lx(L1, i1), y1 = cart_ly(L1, i1), z1 = cart_lz(L1, i1);
+                const int x3 = cart_lx(L3, i3), y3 = cart_ly(L3, i3), z3 = cart_lz(L3, i3);
+#pragma unroll 1
+                for (int i2 = part * N2 / NPART; i2 < (part + 1) * N2 / NPART; ++i2) {
+                    const int x2 = cart_lx(L2, i2), y2 = cart_ly(L2, i2), z2 = cart_lz(L2, i2);
+                    const double(*tx)[4] = &S.T4[0][((x1 * S2 + x2) * S3 + x3) * S4];
+                    const double(*ty)[4] = &S.T4[1][((y1 * S2 + y2) * S3 + y3) * S4];
+                    const double(*tz)[4] = &S.T4[2][((z1 * S2 + z2) * S3 + z3) * S4];
+                    const double* D24r = &S.D24[i2 * N4];
+                    int i4 = 0;
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const int ad = a[d], bd = b[d], cd = c[d], ed = e[d];
-                    v[d] = S.X[d][ad][bd][cd][ed];
-                    da[d] = 2.0 * alpha * S.X[d][ad + 1][bd][cd][ed];
-                    if (ad) da[d] -= ad * S.X[d][ad - 1][bd][cd][ed];
-                    db[d] = 2.0 * beta * S.X[d][ad][bd + 1][cd][ed];
-                    if (bd) db[d] -= bd * S.X[d][ad][bd - 1][cd][ed];
-                    dc[d] = 2.0 * gamma * S.X[d][ad][bd][cd + 1][ed];
-                    if (cd) dc[d] -= cd * S.X[d][ad][bd][cd - 1][ed];
+                    for (int j4 = 0; j4 <= L4; ++j4)
+#pragma unroll
+                        for (int z4 = 0; z4 <= j4; ++z4, ++i4) {
+                            const double W = d13 * D24r[i4];
+                            const double* X4 = tx[L4 - j4];
+                            const double* Y4 = ty[j4 - z4];
+                            const double* Z4 = tz[z4];
+                            const double yz = W * Y4[0] * Z4[0], xz = W * X4[0] * Z4[0], xy = W * X4[0] * Y4[0];
+                            gA[0] = fma(X4[1], yz, gA[0]);
+                            gA[1] = fma(Y4[1], xz, gA[1]);
+                            gA[2] = fma(Z4[1], xy, gA[2]);
+                            gB[0] = fma(X4[2], yz, gB[0]);
+                            gB[1] = fma(Y4[2], xz, gB[1]);
+                            gB[2] = fma(Z4[2], xy, gB[2]);
+                            gC[0] = fma(X4[3], yz, gC[0]);
+                            gC[1] = fma(Y4[3], xz, gC[1]);
+                            gC[2] = fma(Z4[3], xy, gC[2]);
+                        }
                 }
-                const double yz = W * v[1] * v[2], xz = W * v[0] * v[2], xy = W * v[0] * v[1];
-                gA[0] += da[0] * yz;
-                gA[1] += da[1] * xz;
-                gA[2] += da[2] * xy;
-                gB[0] += db[0] * yz;
-                gB[1] += db[1] * xz;
-                gB[2] += db[2] * xy;
-                gC[0] += dc[0] * yz;
-                gC[1] += dc[1] * xz;
-                gC[2] += dc[2] * xy;
             }
             __syncwarp();
         }

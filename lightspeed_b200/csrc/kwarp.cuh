@@ -22,13 +22,13 @@
 
 namespace lsjk {
 
-// Classes that take this kernel: an f shell and at least 324 Cartesian
-// combinations.
+// Classes that take this kernel: an f shell and at least 100 Cartesian
+// combinations (below, a lane's tables still fit L1).
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool k_warp_class()
 {
     return (L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) &&
-           ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 324;
+           ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
 
 template <int L1, int L2, int L3, int L4>
