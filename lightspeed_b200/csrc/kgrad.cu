@@ -32,7 +32,7 @@ namespace lsjk {
 namespace {
 
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
-constexpr int kGradWarpMin = 324;   // Cartesian combinations from which a class runs a quartet per warp
+constexpr int kGradWarpMin = 100;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).
 __device__ __forceinline__ float grad_threshold(double thr, double dmax)
@@ -61,15 +61,13 @@ __host__ __device__ constexpr bool kgrad_flat()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) <= 27;
 }
 
-// The heaviest classes (at least 324 Cartesian combinations: (dd|pp), (dp|dp)
-// and above; with an f shell, at least 100) run one quartet per warp with the
-// tables in shared memory; the rest one quartet per lane.
+// Classes with at least 100 Cartesian combinations ((pp|pp) has 81, (dp|ds)
+// 108) run one quartet per warp with the tables in shared memory; the rest one
+// quartet per lane.
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool kgrad_warp()
 {
-    constexpr int nc = ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4);
-    // with an f shell from 100 combinations on: a lane's tables would no longer fit L1
-    return nc >= kGradWarpMin || ((L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) && nc >= 100);
+    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin;
 }
 
 // One quartet's derivatives at centres 1, 2 and 3 contracted with the D13 and
