@@ -14,9 +14,10 @@
 //     jobs' sums in registers over the partner-1 entries of a shell segment,
 //     and at the segment's end the parts of an element are added in shared
 //     memory and reach K with one atomic per element.
-// Work order and screens are those of k_exchange (one (prim2, prim4) task per
-// warp; partners 3 outer, partners 1 of each partner 3 in segment order), FP64
-// only, one density per task and sub-slot, partners with one output target.
+// Work order and screens are those of k_exchange (a (prim2, prim4) task per
+// warp, here split into stripes of its partners 3; partners 3 outer, partners 1
+// of each partner 3 in segment order), FP64 only, one density per task and
+// sub-slot, partners with one output target.
 #pragma once
 #include "hermite.cuh"   // cart_lx/ly/lz
 
@@ -30,6 +31,8 @@ __host__ __device__ constexpr bool k_warp_class()
     return (L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) &&
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
+
+constexpr int kKWarpStripes = 4;   // partner-3 stripes of a task (work units per task)
 
 template <int L1, int L2, int L3, int L4>
 struct KWarpShape {
@@ -85,10 +88,13 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
     }
     long nq = 0;
     for (;;) {
-        int tv = 0;
-        if (lane == 0) tv = (int) atomicAdd(A.queue, 1u);
-        tv = __shfl_sync(0xffffffffu, tv, 0);
-        if (tv >= ntask) break;
+        // work unit: a task and one of kKWarpStripes stripes of its partners 3 (the small
+        // f-class task lists of a small molecule still fill the GPU)
+        int unit = 0;
+        if (lane == 0) unit = (int) atomicAdd(A.queue, 1u);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= ntask * kKWarpStripes) break;
+        const int tv = unit / kKWarpStripes, stripe = unit - tv * kKWarpStripes;
         const int sub = tv / ntask1;
         const KTask T = A.tasks[tv - sub * ntask1];
         const int dens = T.grp * kKBatch + sub;
@@ -105,10 +111,10 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
             S.D[t] = A.Dc[dens][(long) (c2 + t / N4) * A.ld4 + c4 + t % N4];
         __syncwarp();
         double* Kc = A.Kc[dens];
-        for (int k3i = 0; k3i < n34; ++k3i) {
+        for (int k3i = stripe; k3i < n34; k3i += kKWarpStripes) {
             const int k3 = s34 + k3i;
             const float b34 = A.b34[k3];
-            if (b34 < thre34 || b12max * b34 < tlo) break;   // the row is in bound order
+            if (b34 < thre34 || b12max * b34 < tlo) break;   // the row (and the stripe) is in bound order
             const double kab34 = A.d34.kab[k3], q = A.d34.p[k3], iq = A.d34.ip[k3];
             const double Qx = A.d34.px[k3], Qy = A.d34.py[k3], Qz = A.d34.pz[k3];
             const double Cx = A.d34.ax[k3], Cy = A.d34.ay[k3], Cz = A.d34.az[k3];
@@ -263,6 +269,7 @@ void launch_k_warp(Context* ctx, const KArgs& A, unsigned grid)
         LSJK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         attr_devices.fetch_or(bit, std::memory_order_acq_rel);
     }
+    grid = std::min<unsigned>(grid * kKWarpStripes, (unsigned) ctx->nsm * 16u);
     kern<<<grid, kKThreads, smem, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
