@@ -32,7 +32,7 @@ namespace lsjk {
 namespace {
 
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
-constexpr int kGradStripes = 4;     // partner-3 stripes of a task in the warp kernel (work units per task)
+constexpr int kGradStripes = 8;     // partner-3 stripes of a task in the warp kernel (work units per task)
 constexpr int kGradWarpMin = 100;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).

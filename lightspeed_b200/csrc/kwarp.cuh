@@ -32,7 +32,7 @@ __host__ __device__ constexpr bool k_warp_class()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
 
-constexpr int kKWarpStripes = 4;   // partner-3 stripes of a task (work units per task)
+constexpr int kKWarpStripes = 8;   // partner-3 stripes of a task (work units per task)
 
 template <int L1, int L2, int L3, int L4>
 struct KWarpShape {
