@@ -812,6 +812,12 @@ def run_fshell(args):
 
     ls.set_precision(ls.PREC_FP64)
     (J, K), ms64 = timed(lambda: build(thre))
+    # the K phase alone (FP64) against the FP64 FMA peak: K flops of one build / its time
+    ls.reset_stats()
+    ls.IntBox.exchange(res, ew, pl, pl, Dt, True, thre, thre)
+    k_flops = ls.flops_split()["k_fp64"]
+    _, ms_k64 = timed(lambda: ls.IntBox.exchange(res, ew, pl, pl, Dt, True, thre, thre).np.copy())
+    peak64 = ls.fma_peak_tflops(True)
     ls.set_precision(ls.PREC_MIXED)
     (Jm, Km), msmx = timed(lambda: build(1e-6))
     ls.set_precision(ls.PREC_FP64)
@@ -840,7 +846,12 @@ def run_fshell(args):
         "data": "synthetic",
         "config": {"workload": "%d H2O (seed 0) / cc-pVTZ J+K build and gradient" % nw, "nao": bas.nao,
                    "ncart": bas.ncart, "thresp": thre, "api": "host (D in, J/K or G out)"},
-        "ms_mixed": msmx, "ms_grad": msg, "cpu_baseline": cpu,
+        "ms_mixed": msmx, "ms_grad": msg, "ms_k_fp64": ms_k64,
+        "roofline": {"bound": "fp64", "kernel": "K build (FP64; f classes in k_exchange_warp)",
+                     "achieved": k_flops / (ms_k64 * 1e-3) / 1e12, "peak": peak64, "unit": "TFLOP/s",
+                     "frac": k_flops / (ms_k64 * 1e-3) / 1e12 / peak64, "traffic": None,
+                     "timing": "host wall clock around the synchronous call (includes D in, K out)"},
+        "cpu_baseline": cpu,
     }
     print(json.dumps(line))
     return 0

@@ -31,7 +31,6 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 LIB = os.path.join(PKG, "liblsjk.so")
 LMAX = 3        # largest shell of the kernels (f)
-GEN_LMAX = 2    # largest shell of the straight-line quartet code; above it the loop form
 
 
 def _mtime(p):
@@ -58,7 +57,7 @@ def gen_sources(force=False):
     kgen = os.path.join(CSRC, "gen_kernels.py")
     jq = os.path.join(CSRC, "generated", "jquartets.cuh")
     if force or _mtime(jq) < _mtime(kgen):
-        _run([sys.executable, kgen, str(GEN_LMAX)], cwd=ROOT)
+        _run([sys.executable, kgen, str(LMAX)], cwd=ROOT)
 
 
 def cuda_units():

@@ -1,7 +1,8 @@
 """Emit the straight-line per-quartet integral code for the J and K kernels.
 
-Writes lightspeed_b200/csrc/generated/quartets.cuh with, for every angular
-momentum class up to LMAX per shell:
+Writes lightspeed_b200/csrc/generated/{jquartets,kquartets_*}.cuh with, for the
+angular momentum classes up to LMAX per shell (every class up to d; above d the
+ones below a size limit, see j_emitted / k_emitted):
 
 * jq_B<LB>_K<LK>: McMurchie-Davidson Hermite integrals R_{tuv} built from the
   scaled Boys values a_n = f (-2 rho)^n F_n(T) by the recursion
@@ -226,26 +227,50 @@ def gen_k(L1, L2, L3, L4):
     return head + pre + "\n".join(em.lines) + "\n}\n"
 
 
+def nherm(L):
+    return (L + 1) * (L + 2) * (L + 3) // 6
+
+
+def ncart(L):
+    return (L + 1) * (L + 2) // 2
+
+
+# Every class with shells up to d is emitted. Above d (f shells) a class is emitted
+# while its code stays small enough to compile and schedule well: J up to J_TERMS
+# (t, u) contraction terms, K below K_COMBOS Cartesian combinations (the larger K
+# classes run the quartet-per-warp kernel). The rest take the loop form.
+GEN_D = 2
+J_TERMS = 3200
+K_COMBOS = 100
+
+
+def j_emitted(LB, LK):
+    return (LB <= 2 * GEN_D + 1 and LK <= 2 * GEN_D) or nherm(LB) * nherm(LK) <= J_TERMS
+
+
+def k_emitted(L1, L2, L3, L4):
+    return max(L1, L2, L3, L4) <= GEN_D or ncart(L1) * ncart(L2) * ncart(L3) * ncart(L4) < K_COMBOS
+
+
 def main():
-    lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 2
+    lmax = int(sys.argv[1]) if len(sys.argv) > 1 else 3
     out_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "generated")
     os.makedirs(out_dir, exist_ok=True)
     head = ["// Generated by lightspeed_b200/csrc/gen_kernels.py -- do not edit.", "#pragma once",
             "#define LSJK_GEN_LMAX %d" % lmax, ""]
     # J: Hermite classes 0..2*lmax, and bra classes one higher (2*lmax+1) for the
     # nuclear gradients (the Hermite potential at a bra pair one order above its class)
+    jcls = [(LB, LK) for LB in range(2 * lmax + 2) for LK in range(2 * lmax + 1) if j_emitted(LB, LK)]
     jparts = list(head)
-    for LB in range(2 * lmax + 2):
-        for LK in range(2 * lmax + 1):
-            jparts.append(gen_j(LB, LK))
-    # classes not emitted here (shells above LMAX) take the loop form
+    for LB, LK in jcls:
+        jparts.append(gen_j(LB, LK))
+    # classes not emitted here take the loop form
     jparts.append('#include "quartet_loops.cuh"')
     jparts.append("template <int LB, int LK> struct JQ : lsjk::JQLoop<LB, LK> {};")
-    for LB in range(2 * lmax + 2):
-        for LK in range(2 * lmax + 1):
-            jparts.append("template <> struct JQ<%d, %d> { template <typename R> __device__ __forceinline__ static void "
-                          "run(const R* a, R X, R Y, R Z, const R* dk, R* jp) { jq_B%d_K%d<R>(a, X, Y, Z, dk, jp); } };"
-                          % (LB, LK, LB, LK))
+    for LB, LK in jcls:
+        jparts.append("template <> struct JQ<%d, %d> { template <typename R> __device__ __forceinline__ static void "
+                      "run(const R* a, R X, R Y, R Z, const R* dk, R* jp) { jq_B%d_K%d<R>(a, X, Y, Z, dk, jp); } };"
+                      % (LB, LK, LB, LK))
     jparts.append("template <int LB, int LK, typename R> __device__ __forceinline__ void jq_dispatch("
                   "const R* a, R X, R Y, R Z, const R* dk, R* jp) { JQ<LB, LK>::run(a, X, Y, Z, dk, jp); }")
     with open(os.path.join(out_dir, "jquartets.cuh"), "w") as fh:
@@ -266,6 +291,8 @@ def main():
             kparts = list(head) + ['#include "kquartets_fwd.cuh"', ""]
             for L3 in range(lmax + 1):
                 for L4 in range(lmax + 1):
+                    if not k_emitted(L1, L2, L3, L4):
+                        continue
                     kparts.append(gen_k(L1, L2, L3, L4))
                     kparts.append("template <> struct KQ<%d, %d, %d, %d> { template <typename R> __device__ "
                                   "__forceinline__ static void run(%s) { kq_%d%d%d%d<R>(%s); } };"

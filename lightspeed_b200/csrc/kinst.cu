@@ -1,19 +1,15 @@
 // Instantiates the K kernels whose partner/indexed classes are (L1, L2) on the
 // bra side (compiled once per LSJK_L1, LSJK_L2 in 0..kLmax by the build). The
-// straight-line quartet code exists for shells up to d; classes with an f
-// shell take the loop form (quartet_loops.cuh).
+// generated header holds the straight-line quartet code of the classes it
+// emits; the others take the loop form (quartet_loops.cuh).
 #ifndef LSJK_L1
 #error "compile with -DLSJK_L1=<L> -DLSJK_L2=<L>"
 #endif
-#if LSJK_L1 <= 2 && LSJK_L2 <= 2
 #define LSJK_STR2(x) #x
 #define LSJK_STR(x) LSJK_STR2(x)
 #define LSJK_KHDR(a, b) LSJK_STR(generated/kquartets_##a##b.cuh)
 #define LSJK_KHDR2(a, b) LSJK_KHDR(a, b)
 #include LSJK_KHDR2(LSJK_L1, LSJK_L2)
-#else
-#include "generated/kquartets_fwd.cuh"
-#endif
 #include "kkernel.cuh"
 
 namespace lsjk {
