@@ -63,12 +63,14 @@ __host__ __device__ constexpr bool kgrad_flat()
 }
 
 // Classes with at least 100 Cartesian combinations ((pp|pp) has 81, (dp|ds)
-// 108) run one quartet per warp with the tables in shared memory; the rest one
-// quartet per lane.
+// 108) or an f shell run one quartet per warp with the tables in shared memory;
+// the rest one quartet per lane.
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool kgrad_warp()
 {
-    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin;
+    // (an f shell: always -- a lane's one-quantum-up tables would not fit L1)
+    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin ||
+           L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2;
 }
 
 // One quartet's derivatives at centres 1, 2 and 3 contracted with the D13 and
