@@ -82,6 +82,7 @@ struct KArgs {
     unsigned long long* qcount;
     int nterm;
     double alpha[4], omega[4];
+    int stripes;                 // k_exchange_warp: partner-3 stripes per task (work units per task)
 };
 
 // Launch the FP64 (fp32 = false) or FP32 (fp32 = true) pass of one class.
@@ -119,6 +120,7 @@ struct KGradArgs {
     // a task with prim2 < prim4 stands for itself and its mirror (1,2,3,4) <-> (3,4,1,2),
     // whose terms are equal: its D24 block enters doubled
     int pairsym;
+    int stripes;                // k_exchange_grad_warp: partner-3 stripes per task
     const double* rys;          // FP64 Rys table block of the rule one quantum up
     const double* asym_t;
     const double* asym_w;

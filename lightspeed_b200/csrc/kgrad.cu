@@ -32,7 +32,7 @@ namespace lsjk {
 namespace {
 
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
-constexpr int kGradStripes = 8;     // partner-3 stripes of a task in the warp kernel (work units per task)
+constexpr int kGradStripesMax = 32;   // partner-3 stripes of a task in the warp kernel (work units per task), at most
 constexpr int kGradWarpMin = 100;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).
@@ -532,12 +532,12 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
     const int lane = threadIdx.x & 31;
     const float thre12 = A.sc->thre12, thre34 = A.sc->thre34;
     for (;;) {
-        // work unit: a task and one of kGradStripes stripes of its partners 3
+        // work unit: a task and one of A.stripes stripes of its partners 3
         int unit = 0;
         if (lane == 0) unit = (int) atomicAdd(A.queue, 1u);
         unit = __shfl_sync(0xffffffffu, unit, 0);
-        if (unit >= ntask * kGradStripes) break;
-        const int t = unit / kGradStripes, stripe = unit - t * kGradStripes;
+        if (unit >= ntask * A.stripes) break;
+        const int t = unit / A.stripes, stripe = unit - t * A.stripes;
         const KTask T = A.tasks[t];
         const int i2 = T.i2, i4 = T.i4;
         const float tlo = grad_threshold((double) A.thr_lo, T.dmax);
@@ -551,7 +551,7 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
         const int s12 = A.r12s[i2], n12 = A.r12l[i2], s34 = A.r34s[i4], n34 = A.r34l[i4];
         const float b12max = A.b12[s12];
         double gB[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
-        for (int k = stripe; k < n34; k += kGradStripes) {
+        for (int k = stripe; k < n34; k += A.stripes) {
             const int k3 = s34 + k;
             const float b34 = A.b34[k3];
             if (b34 < thre34 || b12max * b34 < tlo) break;   // bound order: nothing later passes
@@ -624,8 +624,13 @@ void launch_one(Context* ctx, const KGradArgs& A, long cap)
                 devices.fetch_or(bit, std::memory_order_acq_rel);
             }
         }
-        const unsigned gw = (unsigned) std::min<long>((long) grid * kGradStripes, (long) ctx->nsm * 16);
-        kern<<<gw, 128, smem, ctx->stream>>>(A);
+        // stripes per task: at least 8 (long rows split for the load balance), up to about
+        // 64 work units per SM when the class has few tasks
+        KGradArgs B = A;
+        const long want = 64L * ctx->nsm;
+        B.stripes = (int) std::max<long>(8, std::min<long>(kGradStripesMax, (want + cap - 1) / std::max(1L, cap)));
+        const unsigned gw = (unsigned) std::min<long>((cap * B.stripes + 3) / 4, (long) ctx->nsm * 16);
+        kern<<<gw, 128, smem, ctx->stream>>>(B);
     } else
         k_exchange_grad<L1, L2, L3, L4><<<grid, 128, 0, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());

@@ -585,7 +585,7 @@ void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
             // heavy f classes: a quartet per warp (partners with one output target)
             if (!A.gc) {
                 B.nsub = per_group;
-                launch_k_warp<L1, L2, L3, L4>(ctx, B, grid_for(B.nsub));
+                launch_k_warp<L1, L2, L3, L4>(ctx, B, cap * B.nsub, per_sm);
                 return;
             }
         }

@@ -32,7 +32,7 @@ __host__ __device__ constexpr bool k_warp_class()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
 
-constexpr int kKWarpStripes = 8;   // partner-3 stripes of a task (work units per task)
+constexpr int kKWarpStripesMax = 32;   // partner-3 stripes of a task (work units per task), at most
 
 template <int L1, int L2, int L3, int L4>
 struct KWarpShape {
@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
     const int lane = threadIdx.x & 31;
     const int ntask1 = *A.ntask;
     const int ntask = ntask1 * A.nsub;
+    const int nstripe = A.stripes;
     const double* tab = static_cast<const double*>(A.rys);
     const double* asym_t = static_cast<const double*>(A.asym_t);
     const double* asym_w = static_cast<const double*>(A.asym_w);
@@ -88,13 +89,13 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
     }
     long nq = 0;
     for (;;) {
-        // work unit: a task and one of kKWarpStripes stripes of its partners 3 (the small
+        // work unit: a task and one of A.stripes stripes of its partners 3 (the small
         // f-class task lists of a small molecule still fill the GPU)
         int unit = 0;
         if (lane == 0) unit = (int) atomicAdd(A.queue, 1u);
         unit = __shfl_sync(0xffffffffu, unit, 0);
-        if (unit >= ntask * kKWarpStripes) break;
-        const int tv = unit / kKWarpStripes, stripe = unit - tv * kKWarpStripes;
+        if (unit >= ntask * nstripe) break;
+        const int tv = unit / nstripe, stripe = unit - tv * nstripe;
         const int sub = tv / ntask1;
         const KTask T = A.tasks[tv - sub * ntask1];
         const int dens = T.grp * kKBatch + sub;
@@ -111,7 +112,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
             S.D[t] = A.Dc[dens][(long) (c2 + t / N4) * A.ld4 + c4 + t % N4];
         __syncwarp();
         double* Kc = A.Kc[dens];
-        for (int k3i = stripe; k3i < n34; k3i += kKWarpStripes) {
+        for (int k3i = stripe; k3i < n34; k3i += nstripe) {
             const int k3 = s34 + k3i;
             const float b34 = A.b34[k3];
             if (b34 < thre34 || b12max * b34 < tlo) break;   // the row (and the stripe) is in bound order
@@ -259,8 +260,16 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
 }
 
 template <int L1, int L2, int L3, int L4>
-void launch_k_warp(Context* ctx, const KArgs& A, unsigned grid)
+void launch_k_warp(Context* ctx, const KArgs& A0, long units, int per_sm)
 {
+    // stripes per task: at least 8 (long rows split for the load balance), up to about 64
+    // work units per SM when the class has few tasks (the capacity bounds the task count
+    // from above; the screens keep a part of it)
+    KArgs A = A0;
+    const long want = 64L * ctx->nsm;
+    A.stripes = (int) std::max<long>(8, std::min<long>(kKWarpStripesMax, (want + units - 1) / std::max(1L, units)));
+    unsigned grid = (unsigned) std::min<long>((units * A.stripes + kKWarps - 1) / kKWarps,
+                                              (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
     constexpr size_t smem = (size_t) kKWarps * sizeof(KWarpTab<L1, L2, L3, L4>);
     auto kern = k_exchange_warp<L1, L2, L3, L4>;
     static std::atomic<unsigned long long> attr_devices{0};
@@ -269,7 +278,6 @@ void launch_k_warp(Context* ctx, const KArgs& A, unsigned grid)
         LSJK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         attr_devices.fetch_or(bit, std::memory_order_acq_rel);
     }
-    grid = std::min<unsigned>(grid * kKWarpStripes, (unsigned) ctx->nsm * 16u);
     kern<<<grid, kKThreads, smem, ctx->stream>>>(A);
     LSJK_CUDA(cudaGetLastError());
     ctx->stats.kernel_launches++;
