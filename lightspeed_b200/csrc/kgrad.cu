@@ -32,7 +32,8 @@ namespace lsjk {
 namespace {
 
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
-constexpr int kGradStripesMax = 32;   // partner-3 stripes of a task in the warp kernel (work units per task), at most
+constexpr int kGradStripes3 = 32;      // partner-3 stripes of a task in the warp kernel, at most
+constexpr int kGradStripesMax = 256;  // work units per task, at most (beyond 32: partner-1 stripes too)
 constexpr int kGradWarpMin = 100;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).
@@ -537,7 +538,9 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
         if (lane == 0) unit = (int) atomicAdd(A.queue, 1u);
         unit = __shfl_sync(0xffffffffu, unit, 0);
         if (unit >= ntask * A.stripes) break;
-        const int t = unit / A.stripes, stripe = unit - t * A.stripes;
+        const int t = unit / A.stripes, su = unit - t * A.stripes;
+        const int ns3 = A.stripes < kGradStripes3 ? A.stripes : kGradStripes3, ns1 = A.stripes / ns3;
+        const int stripe = su % ns3, stripe1 = su / ns3;   // partner-3 stripe, partner-1 stripe
         const KTask T = A.tasks[t];
         const int i2 = T.i2, i4 = T.i4;
         const float tlo = grad_threshold((double) A.thr_lo, T.dmax);
@@ -551,7 +554,7 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
         const int s12 = A.r12s[i2], n12 = A.r12l[i2], s34 = A.r34s[i4], n34 = A.r34l[i4];
         const float b12max = A.b12[s12];
         double gB[3] = {0, 0, 0}, gD[3] = {0, 0, 0};
-        for (int k = stripe; k < n34; k += A.stripes) {
+        for (int k = stripe; k < n34; k += ns3) {
             const int k3 = s34 + k;
             const float b34 = A.b34[k3];
             if (b34 < thre34 || b12max * b34 < tlo) break;   // bound order: nothing later passes
@@ -565,7 +568,7 @@ __global__ void __launch_bounds__(128) k_exchange_grad_warp(const __grid_constan
             }
             const int c3 = A.cart34[k3], atomC = A.atom34[k3], K3 = A.pidx34[k3];
             double gC[3] = {0, 0, 0};
-            for (int j = 0; j < n12; ++j) {
+            for (int j = stripe1; j < n12; j += ns1) {
                 const int e = s12 + j;
                 const float b12 = A.b12[e];
                 if (b12 < thre12 || b12 * b34 < tlo) break;
@@ -624,11 +627,13 @@ void launch_one(Context* ctx, const KGradArgs& A, long cap)
                 devices.fetch_or(bit, std::memory_order_acq_rel);
             }
         }
-        // stripes per task: at least 8 (long rows split for the load balance), up to about
-        // 64 work units per SM when the class has few tasks
+        // work units per task: at least 8 partner-3 stripes (long rows split for the load
+        // balance), up to about 64 units per SM when the class has few tasks (up to 32
+        // partner-3 stripes, then partner-1 stripes as well)
         KGradArgs B = A;
         const long want = 64L * ctx->nsm;
         B.stripes = (int) std::max<long>(8, std::min<long>(kGradStripesMax, (want + cap - 1) / std::max(1L, cap)));
+        if (B.stripes > kGradStripes3) B.stripes -= B.stripes % kGradStripes3;   // whole partner-1 stripes
         const unsigned gw = (unsigned) std::min<long>((cap * B.stripes + 3) / 4, (long) ctx->nsm * 16);
         kern<<<gw, 128, smem, ctx->stream>>>(B);
     } else

@@ -32,7 +32,8 @@ __host__ __device__ constexpr bool k_warp_class()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
 
-constexpr int kKWarpStripesMax = 32;   // partner-3 stripes of a task (work units per task), at most
+constexpr int kKWarpStripes3 = 32;     // partner-3 stripes of a task, at most
+constexpr int kKWarpStripesMax = 256;  // work units per task, at most (beyond 32: partner-1 segment stripes too)
 
 template <int L1, int L2, int L3, int L4>
 struct KWarpShape {
@@ -67,6 +68,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
     const int ntask1 = *A.ntask;
     const int ntask = ntask1 * A.nsub;
     const int nstripe = A.stripes;
+    const int ns3 = nstripe < kKWarpStripes3 ? nstripe : kKWarpStripes3, ns1 = nstripe / ns3;
     const double* tab = static_cast<const double*>(A.rys);
     const double* asym_t = static_cast<const double*>(A.asym_t);
     const double* asym_w = static_cast<const double*>(A.asym_w);
@@ -95,7 +97,8 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
         if (lane == 0) unit = (int) atomicAdd(A.queue, 1u);
         unit = __shfl_sync(0xffffffffu, unit, 0);
         if (unit >= ntask * nstripe) break;
-        const int tv = unit / nstripe, stripe = unit - tv * nstripe;
+        const int tv = unit / nstripe, su = unit - tv * nstripe;
+        const int stripe = su % ns3, stripe1 = su / ns3;   // partner-3 stripe, partner-1 segment stripe
         const int sub = tv / ntask1;
         const KTask T = A.tasks[tv - sub * ntask1];
         const int dens = T.grp * kKBatch + sub;
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
             S.D[t] = A.Dc[dens][(long) (c2 + t / N4) * A.ld4 + c4 + t % N4];
         __syncwarp();
         double* Kc = A.Kc[dens];
-        for (int k3i = stripe; k3i < n34; k3i += nstripe) {
+        for (int k3i = stripe; k3i < n34; k3i += ns3) {
             const int k3 = s34 + k3i;
             const float b34 = A.b34[k3];
             if (b34 < thre34 || b12max * b34 < tlo) break;   // the row (and the stripe) is in bound order
@@ -150,6 +153,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
                 const int e = s12 + j;
                 const float b12 = A.b12[e];
                 const int sg = A.seg12[e];
+                if (ns1 > 1 && sg % ns1 != stripe1) continue;   // another unit's segment
                 const float est = b12 * b34;
                 const bool can = b12 >= thre12 && est >= tlo;
                 if (sg != prev_seg) {
@@ -262,12 +266,14 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
 template <int L1, int L2, int L3, int L4>
 void launch_k_warp(Context* ctx, const KArgs& A0, long units, int per_sm)
 {
-    // stripes per task: at least 8 (long rows split for the load balance), up to about 64
-    // work units per SM when the class has few tasks (the capacity bounds the task count
-    // from above; the screens keep a part of it)
+    // work units per task: at least 8 partner-3 stripes (long rows split for the load
+    // balance), up to about 64 units per SM when the class has few tasks (the capacity
+    // bounds the task count from above; the screens keep a part of it): up to 32
+    // partner-3 stripes, then partner-1 segment stripes as well
     KArgs A = A0;
     const long want = 64L * ctx->nsm;
     A.stripes = (int) std::max<long>(8, std::min<long>(kKWarpStripesMax, (want + units - 1) / std::max(1L, units)));
+    if (A.stripes > kKWarpStripes3) A.stripes -= A.stripes % kKWarpStripes3;   // whole partner-1 stripes
     unsigned grid = (unsigned) std::min<long>((units * A.stripes + kKWarps - 1) / kKWarps,
                                               (long) ctx->nsm * (per_sm > 0 ? per_sm : 16));
     constexpr size_t smem = (size_t) kKWarps * sizeof(KWarpTab<L1, L2, L3, L4>);
