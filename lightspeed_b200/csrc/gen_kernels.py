@@ -270,7 +270,8 @@ def main():
     jparts.append('#include "quartet_loops.cuh"')
     jparts.append("template <int LB, int LK> struct JQ : lsjk::JQLoop<LB, LK> {};")
     for LB, LK in jcls:
-        jparts.append("template <> struct JQ<%d, %d> { template <typename R> __device__ __forceinline__ static void "
+        jparts.append("template <> struct JQ<%d, %d> { static constexpr bool loop = false; "
+                      "template <typename R> __device__ __forceinline__ static void "
                       "run(const R* a, R X, R Y, R Z, const R* dk, R* jp) { jq_B%d_K%d<R>(a, X, Y, Z, dk, jp); } };"
                       % (LB, LK, LB, LK))
     jparts.append("template <int LB, int LK, typename R> __device__ __forceinline__ void jq_dispatch("

@@ -218,10 +218,147 @@ __global__ void __launch_bounds__(kJThreads) k_coulomb(JArgs A)
     }
 }
 
+// The classes without straight-line code (the largest f classes): a bra pair per
+// warp, FP64. For each ket (bound order, all lanes) the lanes build the Hermite
+// integrals R_tuv in a per-warp shared table -- one shell of (t, u, v) at a time,
+// top shell first, in place, as JQLoop does per thread -- and then each lane
+// contracts its bra components t: jp[t] += sum_u R_{t+u} D_u. A thread-per-pair
+// kernel needs the whole table and the accumulators per thread (several KB),
+// which overflow L1 for 128 threads per CTA.
+constexpr int kJWarpPairs = kJThreads / 32;   // bra pairs per CTA
+
+template <int LB, int LK>
+__global__ void __launch_bounds__(kJThreads) k_coulomb_warp(JArgs A)
+{
+    constexpr int L = LB + LK, HB = nherm_of(LB), HK = nherm_of(LK), NT = (HB + 31) / 32;
+    const int S = 4 + A.slots * HK;
+    __shared__ __align__(128) double tab[LSJK_BOYS_NBIN * 8];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ double Rall[kJWarpPairs][nherm_of(L)];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nb = *A.nbra, nk = *A.nket;
+    const int g = blockIdx.z;   // the density (one per CTA z)
+    const int ib = blockIdx.x * kJWarpPairs;
+    const int j0 = blockIdx.y * A.chunk;
+    if (ib >= nb || j0 >= nk) return;
+    if (A.bbound[ib] * A.kbound[j0] < A.thresp) return;
+    if (!stage_bulk(tab, A.boys, sizeof(tab), &mbar, A.status)) return;
+    const int i = ib + warp;
+    if (i >= nb) return;   // (after the CTA-wide staging)
+    double* Rb = Rall[warp];
+    const double p = A.bgeom[4L * i], Px = A.bgeom[4L * i + 1], Py = A.bgeom[4L * i + 2], Pz = A.bgeom[4L * i + 3];
+    const float Bi = A.bbound[i];
+    // this lane's bra components t = lane + 32 k
+    int tx[NT], ty[NT], tz[NT];
+    double jp[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const int t = lane + 32 * k < HB ? lane + 32 * k : 0;
+        int N = 0;
+        while (nherm_of(N) <= t) ++N;
+        int r = t - nherm_of(N - 1), ii = 0;
+        while ((ii + 1) * (ii + 2) / 2 <= r) ++ii;
+        tz[k] = r - ii * (ii + 1) / 2;
+        ty[k] = ii - tz[k];
+        tx[k] = N - ii;
+        jp[k] = 0.0;
+    }
+    long nq = 0;
+    const int j1 = min(j0 + A.chunk, nk);
+    for (int j = j0; j < j1; ++j) {
+        if (Bi * A.kbound[j] < A.thresp) break;   // kets in bound order
+        const double* r = A.krec + (long) j * S;
+        const double q = r[0];
+        const double X = Px - r[1], Y = Py - r[2], Z = Pz - r[3];
+        const double R2 = X * X + Y * Y + Z * Z;
+        const double rs = rsqrt(p + q);
+        const double rho = p * q * (rs * rs);
+        const double* dk = r + 4 + g * HK;
+        ++nq;
+        for (int tm = 0; tm < A.nterm; ++tm) {
+            const double om = A.omega[tm];
+            double d2 = 1.0, f = A.alpha[tm] * rs;
+            if (om != -1.0) {
+                const double w2 = om * om;
+                d2 = w2 / (rho + w2);
+                f *= sqrt(d2);
+            }
+            const double rhoe = rho * d2;
+            double F[L + 1];
+            boys_eval<L, double>(rhoe * R2, tab, F);
+            double a[L + 1];
+            const double m2r = -2.0 * rhoe;
+            double pw = f;
+#pragma unroll
+            for (int n = 0; n <= L; ++n) {
+                a[n] = pw * F[n];
+                pw *= m2r;
+            }
+            if (lane == 0) Rb[0] = a[L];
+            __syncwarp();
+#pragma unroll 1
+            for (int m = L - 1; m >= 0; --m) {
+#pragma unroll 1
+                for (int N = L - m; N >= 1; --N) {
+                    for (int k = lane; k < (N + 1) * (N + 2) / 2; k += 32) {
+                        int ii = 0;
+                        while ((ii + 1) * (ii + 2) / 2 <= k) ++ii;
+                        const int v = k - ii * (ii + 1) / 2, u = ii - v, t = N - ii;
+                        double sv;
+                        if (t > 0) {
+                            sv = X * Rb[herm_pos(t - 1, u, v)];
+                            if (t > 1) sv = fma(double(t - 1), Rb[herm_pos(t - 2, u, v)], sv);
+                        } else if (u > 0) {
+                            sv = Y * Rb[herm_pos(t, u - 1, v)];
+                            if (u > 1) sv = fma(double(u - 1), Rb[herm_pos(t, u - 2, v)], sv);
+                        } else {
+                            sv = Z * Rb[herm_pos(t, u, v - 1)];
+                            if (v > 1) sv = fma(double(v - 1), Rb[herm_pos(t, u, v - 2)], sv);
+                        }
+                        Rb[nherm_of(N - 1) + k] = sv;
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) Rb[0] = a[m];
+                __syncwarp();
+            }
+#pragma unroll
+            for (int k = 0; k < NT; ++k) {
+                if (lane + 32 * k >= HB) break;
+                double sv = jp[k];
+                int uk = 0;
+#pragma unroll 1
+                for (int NK = 0; NK <= LK; ++NK)
+#pragma unroll 1
+                    for (int ik = 0; ik <= NK; ++ik)
+#pragma unroll 1
+                        for (int vk = 0; vk <= ik; ++vk, ++uk)
+                            sv = fma(Rb[herm_pos(tx[k] + NK - ik, ty[k] + ik - vk, tz[k] + vk)], dk[uk], sv);
+                jp[k] = sv;
+            }
+            __syncwarp();   // the table is rebuilt for the next term or ket
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const int t = lane + 32 * k;
+        if (t < HB && jp[k] != 0.0) atomicAdd(&A.jbra[g * A.jbra_stride + (long) i * HB + t], jp[k]);
+    }
+    if (lane == 0 && nq) atomicAdd(A.qcount, (unsigned long long) nq);
+}
+
 template <int LB, int LK>
 void launch_j(Context* ctx, const JArgs& A, int nbra_full, int nket_full)
 {
     if (nbra_full == 0 || nket_full == 0) return;
+    if constexpr (JQ<LB, LK>::loop) {
+        // classes without straight-line code: a bra pair per warp, FP64, a density per CTA z
+        dim3 grid((nbra_full + kJWarpPairs - 1) / kJWarpPairs, (nket_full + A.chunk - 1) / A.chunk, A.ng);
+        k_coulomb_warp<LB, LK><<<grid, kJThreads, 0, ctx->stream>>>(A);
+        LSJK_CUDA(cudaGetLastError());
+        ctx->stats.kernel_launches++;
+        return;
+    }
     // one launch for all densities: CTA z takes NG of them over the same ket
     // records (NG = the class's batch when there are that many, else 1)
     constexpr int NGB = j_batch<LB>();

@@ -1,6 +1,7 @@
 // Loop forms of the per-quartet integral code, for the classes the generator
-// does not emit as straight-line code (any shell above d: Hermite classes
-// above 2 * 2 + 1 on the bra or 2 * 2 on the ket, K classes with an f shell).
+// does not emit as straight-line code (the largest classes with an f shell; see
+// gen_kernels.py). The J kernel of those classes builds the same table per warp
+// (k_coulomb_warp); the K ones mostly run k_exchange_warp.
 // They compute the same quantities with the same recursions as the generated
 // functions (gen_kernels.py), over index loops into per-thread arrays, so a
 // class of any angular momentum compiles to a compact kernel:
@@ -27,6 +28,7 @@ __host__ __device__ constexpr int herm_pos(int t, int u, int v)
 
 template <int LB, int LK>
 struct JQLoop {
+    static constexpr bool loop = true;   // the class has no straight-line code
     template <typename R>
     __device__ static void run(const R* __restrict__ a, R X, R Y, R Z, const R* __restrict__ dk,
                                R* __restrict__ jp)
