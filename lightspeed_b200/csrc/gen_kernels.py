@@ -238,11 +238,12 @@ def ncart(L):
 # Every class with shells up to d is emitted. Above d (f shells) a class is emitted
 # while its code stays small enough to compile and schedule well: J up to J_TERMS
 # (t, u) contraction terms, K below K_COMBOS Cartesian combinations (the larger K
-# classes run the quartet-per-warp kernel). The rest take the loop form. (Emitted
-# J classes of 4700 terms and more compiled to 32 registers and 38-97 KB of stack
-# per thread.)
+# classes run the quartet-per-warp kernel). The rest take the loop form, and their
+# J kernel is k_coulomb_warp (a bra pair per warp). Emitted J classes of 4700 terms
+# and more compiled to 32 registers and 38-97 KB of stack per thread; between 1600
+# and 3200 terms the emitted and the warp form measured the same.
 GEN_D = 2
-J_TERMS = 3200
+J_TERMS = 1600
 K_COMBOS = 100
 
 
