@@ -9,7 +9,9 @@ IntBox, which takes any angular momentum) on a water dimer in cc-pVTZ
 * range-separated J and K (erf-attenuated and a two-term operator) at 1e-10;
 * S, T at 1e-12 and V at 1e-10;
 * the J and K gradients at 1e-9 (K: the fully symmetric routine, the mirror
-  halving of two symmetric densities, and the unpromised path)."""
+  halving of two symmetric densities, and the unpromised path);
+* non-symmetric pair lists between cc-pVTZ and cc-pVDZ at 1e-10, and K over
+  merged s exponents within 1e-9 of the exact K."""
 import numpy as np
 import pytest
 
@@ -132,3 +134,49 @@ def test_fshell_exchange_grad(ls, oracle_ok):
     assert np.max(np.abs(G_ab - Gr_ab)) < 1e-9
     G_nosym = ls.IntBox.exchangeGrad(res, ew, pl, A, B, False, False, False, 1e-14, 1e-14).np
     assert np.max(np.abs(G_nosym - Gr_ab)) < 1e-9
+
+
+def test_fshell_mixed_basis(ls, oracle_ok):
+    """Non-symmetric pair lists between cc-pVTZ (f) and cc-pVDZ on the same dimer:
+    J and K with a rectangular and a symmetric density against the oracle."""
+    from lightspeed_b200.geometry import water_cluster
+    mol = water_cluster(2, seed=1)
+    b1 = ls.Basis.from_gbs_file(mol, "cc-pvtz")
+    b2 = ls.Basis.from_gbs_file(mol, "cc-pvdz")
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    p11 = ls.PairList.build_schwarz(b1, b1, True, 1e-14)
+    p12 = ls.PairList.build_schwarz(b1, b2, False, 1e-14)
+    r1, r2 = ref.RefBasis(ref.prim_arrays(b1)), ref.RefBasis(ref.prim_arrays(b2))
+    rp11 = ref.RefPairs(r1, r1, True, 1e-14)
+    rp12 = ref.RefPairs(r1, r2, False, 1e-14)
+    rng = np.random.default_rng(13)
+    X = rng.standard_normal((b1.nao, 8)) / np.sqrt(b1.nao)
+    Y = rng.standard_normal((b2.nao, 8)) / np.sqrt(b2.nao)
+    D12 = X @ Y.T
+    J = ls.IntBox.coulomb(res, ew, p11, p12, ls.Tensor.array(D12), 1e-14, 1e-14).np
+    assert np.max(np.abs(J - ref.coulomb(rp11, rp12, D12, 1e-14, 1e-14))) < 1e-10
+    D22 = Y @ Y.T
+    K = ls.IntBox.exchange(res, ew, p12, p12, ls.Tensor.array(D22), True, 1e-14, 1e-14).np
+    assert np.max(np.abs(K - ref.exchange(rp12, rp12, D22, True, 1e-14, 1e-14))) < 1e-10
+
+
+def test_fshell_merged_exponents(ls, oracle_ok):
+    """K over merged s exponents (cc-pVTZ repeats s exponents across contracted
+    shells; the twin classes with an f shell run the two-target kernels): within
+    1e-9 of the oracle's exact K, symmetric and non-symmetric."""
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    D, Dn = _densities(bas, 14)
+    ls.set_merge(True)
+    try:
+        K = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(D), True, 1e-14, 1e-14).np
+        Kn = ls.IntBox.exchange(res, ew, pl, pl, ls.Tensor.array(Dn), False, 1e-14, 1e-14).np
+    finally:
+        ls.set_merge(False)
+    assert np.max(np.abs(K - ref.exchange(rp, rp, D, True, 1e-14, 1e-14))) < 1e-9
+    assert np.max(np.abs(Kn - ref.exchange(rp, rp, Dn, False, 1e-14, 1e-14))) < 1e-9
