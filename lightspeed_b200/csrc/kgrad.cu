@@ -34,7 +34,6 @@ namespace {
 constexpr double kTwoPi52G = 34.986836655249725693;   // 2 pi^(5/2)
 constexpr int kGradStripes3 = 32;      // partner-3 stripes of a task in the warp kernel, at most
 constexpr int kGradStripesMax = 256;  // work units per task, at most (beyond 32: partner-1 stripes too)
-constexpr int kGradWarpMin = 100;   // Cartesian combinations from which a class runs a quartet per warp
 
 // Smallest float x with double(x) * dmax >= thr (as in the K kernel).
 __device__ __forceinline__ float grad_threshold(double thr, double dmax)
@@ -63,15 +62,13 @@ __host__ __device__ constexpr bool kgrad_flat()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) <= 27;
 }
 
-// Classes with at least 100 Cartesian combinations ((pp|pp) has 81, (dp|ds)
-// 108) or an f shell run one quartet per warp with the tables in shared memory;
-// the rest one quartet per lane.
+// Every class that is not light runs one quartet per warp with the tables in
+// shared memory (with work units of partner-3 stripes this measured faster than a
+// quartet per lane for every such class); the light ones one quartet per lane.
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool kgrad_warp()
 {
-    // (an f shell: always -- a lane's one-quantum-up tables would not fit L1)
-    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= kGradWarpMin ||
-           L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2;
+    return !kgrad_flat<L1, L2, L3, L4>();
 }
 
 // One quartet's derivatives at centres 1, 2 and 3 contracted with the D13 and
