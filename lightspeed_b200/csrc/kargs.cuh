@@ -83,6 +83,7 @@ struct KArgs {
     int nterm;
     double alpha[4], omega[4];
     int stripes;                 // k_exchange_warp: partner-3 stripes per task (work units per task)
+    int split_hi;                // this is the FP64 pass of a mixed build (estimate >= thredp only)
 };
 
 // Launch the FP64 (fp32 = false) or FP32 (fp32 = true) pass of one class.

@@ -400,6 +400,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                     }
                     A.thr_lo = two_pass ? thredp : thresp;
                     A.thr_hi = inf;
+                    A.split_hi = two_pass ? 1 : 0;
                     A.rys = ctx->rys64.p + kRysOffset[NR];
                     A.asym_t = ctx->rys_asym64.p + NR * LSJK_RYS_NMAX;
                     A.asym_w = ctx->rys_asym64.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;
@@ -450,6 +451,7 @@ void exchange_build(Context* ctx, const Ewald& ew, const PairList* pl12, const P
                         A.queue = queue + kNCombo + c;
                         A.thr_lo = thresp;
                         A.thr_hi = thredp;
+                        A.split_hi = 0;
                         A.rys = ctx->rys32.p + kRysOffset[NR];
                         A.asym_t = ctx->rys_asym32.p + NR * LSJK_RYS_NMAX;
                         A.asym_w = ctx->rys_asym32.p + (LSJK_RYS_NMAX + 1) * LSJK_RYS_NMAX + NR * LSJK_RYS_NMAX;

@@ -581,9 +581,10 @@ void launch_k(Context* ctx, const KArgs& A, long cap, bool fp32)
             launch_k_gc<L1, L2, L3, L4, float, 1>(ctx, B, grid_for(B.nsub));
         }
     } else {
-        if constexpr (k_warp_class<L1, L2, L3, L4>()) {
-            // heavy f classes: a quartet per warp (partners with one output target)
-            if (!A.gc) {
+        if constexpr (k_warp_class<L1, L2, L3, L4>() || k_warp_class_hi<L1, L2, L3, L4>()) {
+            // heavy classes: a quartet per warp (partners with one output target; over
+            // merged twins only s-type partners can carry two)
+            if ((k_warp_class<L1, L2, L3, L4>() || A.split_hi) && (!A.gc || (L1 != 0 && L3 != 0))) {
                 B.nsub = per_group;
                 launch_k_warp<L1, L2, L3, L4>(ctx, B, cap * B.nsub, per_sm);
                 return;

@@ -32,6 +32,15 @@ __host__ __device__ constexpr bool k_warp_class()
            ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 100;
 }
 
+// The heavy classes without an f shell (at least 324 combinations) take it for the
+// FP64 pass of a mixed build, whose few tasks (those that reach thredp) a quartet
+// per lane spreads too thinly; their full FP64 builds stay a quartet per lane.
+template <int L1, int L2, int L3, int L4>
+__host__ __device__ constexpr bool k_warp_class_hi()
+{
+    return ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4) >= 324;
+}
+
 constexpr int kKWarpStripes3 = 32;     // partner-3 stripes of a task, at most
 constexpr int kKWarpStripesMax = 256;  // work units per task, at most (beyond 32: partner-1 segment stripes too)
 
