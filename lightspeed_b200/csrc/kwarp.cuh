@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
     const double thr_lo = (double) A.thr_lo, thr_hi = (double) A.thr_hi;
 
     // this lane's jobs: element o = job / P (i1 = o / N3, i3 = o % N3), i2 range part = job % P
-    int jx[NJL][3], jy[NJL][3], jz[NJL][3];   // Cartesian exponents of shells 1 and 3, and o
+    int jx[NJL][2], jy[NJL][2], jz[NJL][2];   // Cartesian exponents of shells 1 and 3
     int j2lo[NJL], j2hi[NJL];
 #pragma unroll
     for (int k = 0; k < NJL; ++k) {
@@ -94,7 +94,6 @@ __global__ void __launch_bounds__(kKThreads) k_exchange_warp(const __grid_consta
         const int i1 = o / N3, i3 = o % N3;
         jx[k][0] = cart_lx(L1, i1); jy[k][0] = cart_ly(L1, i1); jz[k][0] = cart_lz(L1, i1);
         jx[k][1] = cart_lx(L3, i3); jy[k][1] = cart_ly(L3, i3); jz[k][1] = cart_lz(L3, i3);
-        jx[k][2] = o;
         j2lo[k] = job < NJOB ? part * N2 / P : 0;
         j2hi[k] = job < NJOB ? (part + 1) * N2 / P : 0;
     }

@@ -11,7 +11,8 @@ IntBox, which takes any angular momentum) on a water dimer in cc-pVTZ
 * the J and K gradients at 1e-9 (K: the fully symmetric routine, the mirror
   halving of two symmetric densities, and the unpromised path);
 * non-symmetric pair lists between cc-pVTZ and cc-pVDZ at 1e-10, and K over
-  merged s exponents within 1e-9 of the exact K."""
+  merged s exponents within 1e-9 of the exact K;
+* six densities in one build and IntBox.eriJ at 1e-10."""
 import numpy as np
 import pytest
 
@@ -180,3 +181,36 @@ def test_fshell_merged_exponents(ls, oracle_ok):
         ls.set_merge(False)
     assert np.max(np.abs(K - ref.exchange(rp, rp, D, True, 1e-14, 1e-14))) < 1e-9
     assert np.max(np.abs(Kn - ref.exchange(rp, rp, Dn, False, 1e-14, 1e-14))) < 1e-9
+
+
+def test_fshell_multi_density_and_eriJ(ls, oracle_ok):
+    """Six non-symmetric densities in one build (J: CTA z-slices; K: density groups
+    and sub-slots, the warp kernel included) and IntBox.eriJ over the same basis,
+    against the oracle."""
+    mol, bas = _dimer(ls)
+    res = ls.ResourceList.build()
+    ew = ls.Ewald.coulomb()
+    pl = ls.PairList.build_schwarz(bas, bas, True, 1e-14)
+    rb = ref.RefBasis(ref.prim_arrays(bas))
+    rp = ref.RefPairs(rb, rb, True, 1e-14)
+    rng = np.random.default_rng(21)
+    Dn = []
+    for _ in range(6):
+        X = rng.standard_normal((bas.nao, 4)) / np.sqrt(bas.nao)
+        Y = rng.standard_normal((bas.nao, 4)) / np.sqrt(bas.nao)
+        Dn.append(X @ Y.T)
+    ls.set_precision(ls.PREC_FP64)
+    try:
+        Ds = [ls.Tensor.array(D) for D in Dn]
+        Jm = ls.IntBox.coulombMulti(res, ew, pl, pl, Ds, 1e-14, 1e-14)
+        Km = ls.IntBox.exchangeMulti(res, ew, pl, pl, Ds, False, 1e-14, 1e-14)
+        C = rng.standard_normal((bas.nao, 3)) / np.sqrt(bas.nao)
+        A = ls.Tensor.array(C)
+        I = ls.IntBox.eriJ(res, ew, pl, pl, A, A, A, A, 1e-14, 1e-14).np.copy()
+    finally:
+        ls.set_precision(ls.PREC_MIXED)
+    for D, J, K in zip(Dn, Jm, Km):
+        assert np.max(np.abs(J.np - ref.coulomb(rp, rp, D, 1e-14, 1e-14))) < 1e-10
+        assert np.max(np.abs(K.np - ref.exchange(rp, rp, D, False, 1e-14, 1e-14))) < 1e-10
+    Iref = ref.eri_j(rp, rp, C, C, C, C, 1e-14, 1e-14, True, True, True)
+    assert np.max(np.abs(I - Iref)) < 1e-10
