@@ -24,13 +24,14 @@
 namespace lsjk {
 
 // Classes that take this kernel: an f shell and at least 100 Cartesian
-// combinations (below, a lane's tables still fit L1), and (dd|dd) (1296
-// combinations: its straight-line quartet spills ~29 KB per lane in FP64).
+// combinations (below, a lane's tables still fit L1), and the classes of at
+// least 600 ((dd|dd), (dd|dp) and the like: their straight-line FP64 quartets
+// spill 5-29 KB per lane; from 324 on the FP64 build measured slower).
 template <int L1, int L2, int L3, int L4>
 __host__ __device__ constexpr bool k_warp_class()
 {
     constexpr int nc = ncart_of(L1) * ncart_of(L2) * ncart_of(L3) * ncart_of(L4);
-    return ((L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) && nc >= 100) || nc >= 1000;
+    return ((L1 > 2 || L2 > 2 || L3 > 2 || L4 > 2) && nc >= 100) || nc >= 600;
 }
 
 // The heavy classes without an f shell (at least 324 combinations) take it for the
