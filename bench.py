@@ -29,7 +29,7 @@ sys.path.insert(0, ROOT)
 METRIC = "J+K ms/iter & quartets/s: mixed vs FP64 GPU at |ΔE|≤1e-6 Eh; CPU ref alongside"
 THRE = 1.0e-14
 THREDP = 1.0e-5
-K_TRAFFIC_C40 = 4.614e9   # ncu dram__bytes_read.sum + dram__bytes_write.sum, FP64 K build of C40H82
+K_TRAFFIC_C40 = 0.6423e9  # ncu dram__bytes_read.sum + dram__bytes_write.sum, FP64 K build of C40H82
 SAMPLE_CARBONS = 8        # CPU baseline sample: C8H18 / cc-pVDZ, full J+K
 
 
