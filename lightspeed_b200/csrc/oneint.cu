@@ -14,6 +14,7 @@
 // symmetric pair-list consumers). The pure transform follows on the device.
 #include "engine.cuh"
 #include "hermite.cuh"
+#include "quartet_loops.cuh"   // herm_pos
 
 namespace lsjk {
 
@@ -42,45 +43,40 @@ struct OneArgs {
 // from the Boys values F_0..F_L, by the downward recursion in n of
 //   R^n_{t+1,u,v} = t R^{n+1}_{t-1,u,v} + X R^{n+1}_{t,u,v}   (likewise u, v),
 //   R^n_{000} = (-2a)^n F_n,
-// keeping two levels. Result in R[t][u][v].
+// in place over one array in shell-major order (herm_pos): level n from level
+// n + 1, top shell first, so the shells a step reads still hold level n + 1.
 template <int L>
-__device__ void hermite_R(double a, double X, double Y, double Z, const double* F, double (*R)[L + 1][L + 1])
+__device__ void hermite_R(double a, double X, double Y, double Z, const double* F, double* R)
 {
-    constexpr int V = L + 1;
-    double nxt[V][V][V];
-    double pw = 1.0;
     double f[L + 1];
+    double pw = 1.0;
     for (int n = 0; n <= L; ++n) {
         f[n] = pw * F[n];
         pw *= -2.0 * a;
     }
-    // level L: only R_000
-    nxt[0][0][0] = f[L];
-    for (int n = L - 1; n >= 0; --n) {
-        const int top = L - n;
-        for (int t = 0; t <= top; ++t)
-            for (int u = 0; u + t <= top; ++u)
-                for (int v = 0; v + u + t <= top; ++v) {
+    R[0] = f[L];
+    for (int m = L - 1; m >= 0; --m) {
+        for (int N = L - m; N >= 1; --N) {
+            int k = nherm_of(N - 1);
+            for (int i = 0; i <= N; ++i)
+                for (int v = 0; v <= i; ++v, ++k) {
+                    const int t = N - i, u = i - v;
                     double s;
-                    if (t + u + v == 0) {
-                        s = f[n];
-                    } else if (t > 0) {
-                        s = X * nxt[t - 1][u][v];
-                        if (t > 1) s += (t - 1) * nxt[t - 2][u][v];
+                    if (t > 0) {
+                        s = X * R[herm_pos(t - 1, u, v)];
+                        if (t > 1) s += (t - 1) * R[herm_pos(t - 2, u, v)];
                     } else if (u > 0) {
-                        s = Y * nxt[t][u - 1][v];
-                        if (u > 1) s += (u - 1) * nxt[t][u - 2][v];
+                        s = Y * R[herm_pos(t, u - 1, v)];
+                        if (u > 1) s += (u - 1) * R[herm_pos(t, u - 2, v)];
                     } else {
-                        s = Z * nxt[t][u][v - 1];
-                        if (v > 1) s += (v - 1) * nxt[t][u][v - 2];
+                        s = Z * R[herm_pos(t, u, v - 1)];
+                        if (v > 1) s += (v - 1) * R[herm_pos(t, u, v - 2)];
                     }
-                    R[t][u][v] = s;
+                    R[k] = s;
                 }
-        for (int t = 0; t <= top; ++t)
-            for (int u = 0; u + t <= top; ++u)
-                for (int v = 0; v + u + t <= top; ++v) nxt[t][u][v] = R[t][u][v];
+        }
+        R[0] = f[m];
     }
-    if (L == 0) R[0][0][0] = f[0];
 }
 
 template <int LA, int LB, int KIND>
@@ -135,12 +131,10 @@ __global__ void __launch_bounds__(128) k_oneint(const __grid_constant__ OneArgs 
                 }
             }
     } else {
-        constexpr int L = LA + LB, V = L + 1;
-        double Rs[V][V][V];
-        for (int t = 0; t < V; ++t)
-            for (int u = 0; u < V; ++u)
-                for (int v = 0; v < V; ++v) Rs[t][u][v] = 0.0;
-        double R[V][V][V];
+        constexpr int L = LA + LB, H = nherm_of(L);
+        double Rs[H];
+        for (int k = 0; k < H; ++k) Rs[k] = 0.0;
+        double R[H];
         double F[L + 1];
         for (int C = 0; C < A.natom; ++C) {
             const double Zc = A.xyzc[4 * C + 3];
@@ -158,9 +152,7 @@ __global__ void __launch_bounds__(128) k_oneint(const __grid_constant__ OneArgs 
                 boys_eval<L, double>(p * d2 * R2, A.boys, F);
                 hermite_R<L>(p * d2, X, Y, Z, F, R);
                 const double c = -Zc * al * f * 2.0 * kPi * ip;
-                for (int t = 0; t < V; ++t)
-                    for (int u = 0; u + t < V; ++u)
-                        for (int v = 0; v + u + t < V; ++v) Rs[t][u][v] += c * R[t][u][v];
+                for (int k = 0; k < H; ++k) Rs[k] += c * R[k];
             }
         }
 #pragma unroll
@@ -173,7 +165,7 @@ __global__ void __launch_bounds__(128) k_oneint(const __grid_constant__ OneArgs 
                 for (int t = 0; t <= ax + bx; ++t)
                     for (int u = 0; u <= ay + by; ++u)
                         for (int w = 0; w <= az + bz; ++w)
-                            v += E.v[0][ax][bx][t] * E.v[1][ay][by][u] * E.v[2][az][bz][w] * Rs[t][u][w];
+                            v += E.v[0][ax][bx][t] * E.v[1][ay][by][u] * E.v[2][az][bz][w] * Rs[herm_pos(t, u, w)];
                 out[i][j] = v;
             }
     }
